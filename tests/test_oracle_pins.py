@@ -1,0 +1,250 @@
+"""Pins the FP64 oracle to the reference's own known-answer and identity tests.
+
+Each test names the reference test it restates (paths relative to the beamax
+project root).  Random inputs are re-seeded with NumPy because the reference's
+JAX threefry streams cannot be reproduced without JAX.
+"""
+
+import numpy as np
+import pytest
+
+from oracle import msgb as om
+
+
+def _wpt(num_levels, N, boxes, bar=None, windowing="rectangular", redundancy=2):
+    bar = bar or (1,) * len(N)
+    dec = om.Decomp(num_levels, N, boxes, bar)
+    return om.Wpt(dec, redundancy, windowing)
+
+
+@pytest.mark.parametrize(
+    "N, lengths, retained",
+    [((2048,), (32, 64, 128), (4, 6, 12)), ((256, 256), (4, 8, 16), (16, 60, 240))],
+)
+def test_three_level_tiling(N, lengths, retained):
+    """tests/test_decomposition.py:113-130."""
+    dec = om.Decomp(3, N, (4, 8, 16), (1,) * len(N))
+    assert tuple(int(x) for x in dec.box_lengths) == lengths
+    assert tuple(int(x) for x in dec.num_boxes_ndim) == retained
+
+
+@pytest.mark.parametrize("N", [(64, 64), (32, 32)])
+def test_rejects_short_boxes(N):
+    """tests/test_decomposition.py:133-141."""
+    with pytest.raises(ValueError, match="at least 2 Fourier samples"):
+        om.Decomp(3, N, (4, 8, 16), (1, 1))
+
+
+def test_config3_tiling_as_stated_is_rejected_and_corrected_tiling_is_valid():
+    """1024^2 with boxes (4,8,16,32,64) has a level-0 box length of 1."""
+    with pytest.raises(ValueError, match="at least 2 Fourier samples"):
+        om.Decomp(5, (1024, 1024), (4, 8, 16, 32, 64), (1, 1))
+    # 5 levels with (2,4,8,16,32): a 2x2 level-0 grid leaves nothing inside
+    # level 1's lattice to cut out, so the centre count check
+    # (decomposition.py:529-534) rejects it as well.
+    with pytest.raises(ValueError, match="centre count"):
+        om.Decomp(5, (1024, 1024), (2, 4, 8, 16, 32), (1, 1))
+    dec = om.Decomp(4, (1024, 1024), (4, 8, 16, 32), (1, 1))
+    assert tuple(int(x) for x in dec.box_lengths) == (4, 8, 16, 32)
+    assert tuple(int(x) for x in dec.num_boxes_ndim) == (16, 60, 240, 960)
+
+
+@pytest.mark.parametrize("nl", [1, 2])
+@pytest.mark.parametrize("N", [(128,), (128, 128), (256, 128)])
+def test_decomp_is_dyadic(nl, N):
+    """tests/test_decomposition.py:94-110."""
+    dec = om.Decomp(nl, N, tuple(2 ** (l + 2) for l in range(nl)), (1,) * len(N))
+    for i in range(1, nl):
+        assert dec.box_lengths[i] == 2 * dec.box_lengths[i - 1]
+
+
+@pytest.mark.parametrize("windowing", ["rectangular", "rectangular_mirror"])
+@pytest.mark.parametrize("N,bar", [((128,), (1,)), ((128, 128), (1, 1)), ((256, 128), (2, 1))])
+def test_partition_of_unity(N, bar, windowing):
+    """tests/test_ms_filters.py:60-92: sum g*h == 1, 0 <= g <= 1."""
+    dec = om.Decomp(2, N, (4, 8), bar)
+    g, h = om.compute_gh_filters(dec, 2, windowing)
+    assert np.allclose(np.sum(g * h, axis=0), 1.0, atol=1e-15, rtol=0)
+    assert np.all(g >= 0) and np.all(g <= 1)
+
+
+ROUNDTRIP = [
+    (1, (128,), (4,), (1,), "rectangular"),
+    (2, (128,), (4, 8), (1,), "rectangular_mirror"),
+    (2, (128, 128), (4, 8), (1, 1), "rectangular"),
+    (2, (256, 128), (4, 8), (1, 1), "rectangular_mirror"),
+    (2, (256, 128), (4, 8), (2, 1), "rectangular"),
+    (1, (128, 512), (4,), (1, 4), "rectangular_mirror"),
+]
+
+
+@pytest.mark.parametrize("nl,N,boxes,bar,windowing", ROUNDTRIP)
+def test_inverse_forward_identity(nl, N, boxes, bar, windowing):
+    """tests/test_transforms.py:108-118 and 121-135."""
+    w = _wpt(nl, N, boxes, bar, windowing)
+    rng = np.random.default_rng(0)
+    f = rng.standard_normal(N) + 1j * rng.standard_normal(N)
+    assert np.allclose(w.inverse(w.forward(f)), f, atol=1e-13, rtol=0)
+    c = rng.standard_normal(w.total_coeffs)
+    f1 = w.inverse(c)
+    assert np.allclose(w.inverse(w.forward(f1)), f1, atol=1e-13, rtol=0)
+
+
+def test_redundancy_one_anisotropic_roundtrip():
+    """tests/test_transforms.py:78-86."""
+    w = _wpt(2, (64, 32), (4, 8), (2, 1), "rectangular", redundancy=1)
+    f = np.random.default_rng(91).standard_normal((64, 32))
+    assert np.allclose(w.inverse(w.forward(f)), f, atol=1e-12, rtol=1e-12)
+
+
+def test_forward_rejects_unwindowed():
+    """tests/test_transforms.py:64-75."""
+    w = _wpt(1, (64,), (4,), windowing="none")
+    with pytest.raises(ValueError, match="does not support windowing='none'"):
+        w.forward(np.ones(64))
+
+
+@pytest.mark.parametrize("nl,N", [(1, (128,)), (2, (128, 128)), (2, (256, 128))])
+def test_single_coefficient_equals_frame(nl, N):
+    """tests/test_frames.py:359-411."""
+    w = _wpt(nl, N, tuple(2 ** (l + 2) for l in range(nl)), windowing="rectangular_mirror")
+    dec = w.dyadic_decomp
+    rng = np.random.default_rng(1)
+    for idx in rng.integers(0, w.total_coeffs, size=3):
+        c = np.zeros(w.total_coeffs)
+        c[idx] = 1.0
+        got = w.inverse(c, "fourier")
+        lvl, mi = om.find_tensor_and_multiindex([idx], om.coeff_shapes(w))
+        box = mi[0, 0] + w.boxes_cumsum[lvl[0]]
+        ref = om.compute_frames(dec, box, mi[1:, 0], dec.fourier_meshgrid, 2, "rectangular_mirror")
+        assert np.allclose(ref, got, atol=1e-14, rtol=1e-12)
+
+
+def test_isotropic_redundancy_two_phases_trivial():
+    """tests/test_frames.py:452-466."""
+    w = _wpt(2, (64, 64), (4, 8))
+    lvl, mi = om.find_tensor_and_multiindex(np.arange(w.total_coeffs), om.coeff_shapes(w))
+    box = mi[0] + np.r_[0, np.cumsum(w.dyadic_decomp.num_boxes_ndim)][lvl]
+    ph = om.compute_frame_phase(w.dyadic_decomp, box, mi[1:].T, 2)
+    assert np.array_equal(ph, np.ones_like(ph))
+
+
+def test_beam_init_equals_frame_atoms():
+    """tests/solvers/test_fwd_solver.py:272-361: sum coeff*GB(t=0) == sum frames."""
+    N = (128, 128)
+    dom = om.Dom(N=N, dx=(1e-4, 1e-4), periodic=(True, True), cfl=0.354, c=1500.0)
+    w = _wpt(2, N, (4, 8))
+    dec = w.dyadic_decomp
+    rng = np.random.default_rng(0)
+    idx = np.unique(rng.integers(0, w.total_coeffs, size=2))
+    manual = 0
+    lvl, mi = om.find_tensor_and_multiindex(idx, om.coeff_shapes(w))
+    for j in range(idx.size):
+        box = mi[0, j] + w.boxes_cumsum[lvl[j]]
+        manual = manual + om.unitary_ifft(om.compute_frames(dec, box, mi[1:, j], dec.fourier_meshgrid, 2, "none"))
+    p0s, M0s, x0s, oms, a0s, modes = om.compute_forward_parameters(idx, w, dom)
+    xt, pt, Mt, At = om.solve_hom_diag(x0s, p0s, M0s, a0s, modes, np.array([0.0]), 1500.0)
+    G = om.gaussian_beam_complex(xt, pt, Mt, At, oms, dom.grid, dom.grid_size, dom.periodic)
+    gb = np.sum(G, axis=-1)[0]
+    assert np.allclose(gb, manual, atol=1e-14, rtol=0)
+
+
+def test_coefficients_dpdt_zero_and_p0_zero():
+    """tests/solvers/test_solver_utils.py:24-92."""
+    N = (128, 64)
+    dom = om.Dom(N=N, dx=(1e-4, 1e-4), periodic=(False, False), c=1500.0)
+    w = _wpt(2, N, (4, 8))
+    f = np.random.default_rng(0).standard_normal(N)
+    z = np.zeros(N)
+    cp, cn = om.compute_coefficients(f, z, "spatial", dom, w)
+    assert np.allclose(cp, cn)
+    cp, cn = om.compute_coefficients(z, f, "spatial", dom, w)
+    assert np.allclose(cp, -cn)
+
+
+def test_coefficients_conjugate_pairs():
+    """tests/solvers/test_solver_utils.py:231-299."""
+    N = (128, 64)
+    dom = om.Dom(N=N, dx=(1e-4, 1e-4), periodic=(False, False), c=1500.0)
+    w = _wpt(2, N, (4, 8), windowing="rectangular_mirror")
+    rng = np.random.default_rng(10)
+    cp, cn = om.compute_coefficients(rng.standard_normal(N), rng.standard_normal(N), "spatial", dom, w)
+    for l in range(2):
+        s, e = w.coeffs_cumsum[l], w.coeffs_cumsum[l + 1]
+        P = cp[s:e].reshape(w.coeff_shapes[l])
+        Q = cn[s:e].reshape(w.coeff_shapes[l])
+        nb = P.shape[0]
+        for b in range(nb):
+            assert np.allclose(P[b], np.conj(Q[nb - b - 1]))
+
+
+def test_top_n_returns_ascending_magnitudes():
+    """tests/solvers/test_msgb_solver_misc.py:515-558 (values 3 then 4)."""
+    idx, vals = om.threshold_top_n(np.array([1.0, 4.0, 2.0, 3.0]), 2)
+    assert np.array_equal(vals, [3.0, 4.0])
+    assert np.array_equal(idx, [3, 1])
+
+
+def test_top_n_tie_rule():
+    """Ties at the threshold keep the higher flat indices (JAX argpartition)."""
+    c = np.array([0.0, 5.0, 0.0, 0.0, 5.0, 1.0])
+    idx, _ = om.threshold_top_n(c, 4)
+    assert list(idx) == [3, 5, 1, 4]
+
+
+def test_oversized_top_n_matches_half_frame_cap():
+    """tests/solvers/test_msgb_solver_misc.py:352-389."""
+    N = (16,)
+    dom = om.Dom(N=N, dx=(1.0 / 16,), periodic=(True,), c=1.0)
+    w = _wpt(1, N, (4,))
+    half = sum((e - s) // 2 for s, e in zip(w.coeffs_cumsum[:-1], w.coeffs_cumsum[1:]))
+    p0 = np.random.default_rng(37).standard_normal(N)
+    sens = dom.grid.reshape(-1, 1)
+    ts = np.linspace(0.0, 0.02, 3)
+    d1, b1 = om.forward(p0, dom, sens, ts, w, half)
+    d2, b2 = om.forward(p0, dom, sens, ts, w, w.total_coeffs)
+    assert b1.idx.shape == (half,)
+    assert np.all(np.abs(b1.a0_unit * b1.coeff) > 0)
+    assert np.allclose(d1, d2, rtol=1e-12, atol=1e-12)
+    assert np.array_equal(b1.idx, b2.idx)
+
+
+def _packet(x, centre, width, cycles):
+    return np.exp(-0.5 * ((x - centre) / width) ** 2) * np.cos(2 * np.pi * cycles * (x - centre))
+
+
+def test_dalembert_1d_forward():
+    """examples/diagnostics/msgb_adjoint_pairing.py:189-199: (P f)(0, t) ~= f(c t)/2."""
+    n = 128
+    dx = 1.0 / n
+    dt = 1.0 / n
+    dom = om.Dom(N=(n,), dx=(dx,), periodic=(False,), c=1.0)
+    w = _wpt(2, (n,), (4, 8))
+    x = dom.grid[..., 0]
+    f = _packet(x, 0.58, 0.075, 24.0)
+    ts = np.arange(n) * dt
+    sens = np.zeros((1, 1))
+    data, _ = om.forward(f, dom, sens, ts, w, 32)
+    ref = 0.5 * _packet(ts, 0.58, 0.075, 24.0)
+    assert om.rel_l2(ref, data[:, 0]) < 2e-2
+
+
+def test_adjoint_dot_product_2d():
+    """Exact transpose: <A p0, d> == <p0, A* d> at round-off."""
+    N = (64, 64)
+    dom = om.Dom(N=N, dx=(1e-4, 1e-4), periodic=(False, False), c=1500.0)
+    w = _wpt(2, N, (4, 8), windowing="rectangular_mirror")
+    rng = np.random.default_rng(3)
+    p0 = rng.standard_normal(N)
+    mask = np.zeros(N)
+    mask[0, :] = 1
+    mask[:, 0] = 1
+    sens = om.sensor_positions_from_mask(dom, mask)
+    ts = dom.generate_time_domain()[::8]
+    bm = om.select_beams(p0, dom, w, 300)
+    Ap = om.forward_hom(bm, dom, sens, ts)
+    d = rng.standard_normal(Ap.shape)
+    q = rng.standard_normal(N)
+    lhs = np.sum(om.forward_hom(om.beams_for(bm.idx, om.compute_coefficients(q, np.zeros(N), "spatial", dom, w, "pos_only")[bm.idx], dom, w), dom, sens, ts) * d)
+    rhs = np.sum(q * om.adjoint(bm, dom, sens, ts, w, d))
+    assert abs(lhs - rhs) <= 1e-12 * max(abs(lhs), abs(rhs))
