@@ -1,0 +1,122 @@
+"""ctypes binding of libmsgb.so (the C ABI declared in include/msgb.h).
+
+The library is loaded from this package directory.  There is no fallback: if
+the shared library is missing or fails to load, every compute entry point
+raises ``RuntimeError``.  Status codes other than ``MSGB_OK`` are raised as
+``RuntimeError`` carrying ``msgb_last_error()``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmsgb.so")
+
+c_i32 = ctypes.c_int32
+c_i64 = ctypes.c_int64
+c_dbl = ctypes.c_double
+c_vp = ctypes.c_void_p
+c_sz = ctypes.c_size_t
+
+STATUS = {0: "OK", 1: "ARG", 2: "WORKSPACE", 3: "CUDA", 4: "UNSUPPORTED", 5: "NONFINITE", 6: "TIMEOUT"}
+
+
+class Problem(ctypes.Structure):
+    _fields_ = [("ndim", c_i32), ("periodic", c_i32 * 3), ("L", c_dbl * 3), ("c", c_dbl),
+                ("nt", c_i64), ("ts", c_vp), ("ns", c_i64), ("sensors", c_vp)]
+
+
+class BeamSet(ctypes.Structure):
+    _fields_ = [("n", c_i64), ("x0", c_vp), ("p0", c_vp), ("alpha", c_vp), ("a0", c_vp),
+                ("omega", c_vp)]
+
+
+class SumOpts(ctypes.Structure):
+    _fields_ = [("cutoff", c_dbl), ("eval_count", c_vp)]
+
+
+class MswptDesc(ctypes.Structure):
+    _fields_ = [("ndim", c_i32), ("N", c_i32 * 3), ("aspect", c_i32 * 3), ("redundancy", c_i32),
+                ("num_levels", c_i32), ("total_boxes", c_i32), ("box_length", c_vp),
+                ("box_level", c_vp), ("centres", c_vp),
+                ("box_shape", c_vp), ("coeffs_cumsum", c_vp), ("boxes_cumsum", c_vp),
+                ("gfilt", c_vp), ("gfilt_offset", c_vp), ("sum_gsquare", c_vp),
+                ("lattice_counts", c_vp), ("lattice_first", c_vp), ("lattice_step", c_vp),
+                ("lattice_offset", c_vp), ("lattice_box", c_vp)]
+
+
+class BeamOut(ctypes.Structure):
+    _fields_ = [("x0", c_vp), ("p0", c_vp), ("alpha", c_vp), ("a0", c_vp), ("omega", c_vp),
+                ("a0_unit", c_vp)]
+
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "msgb_last_error": (ctypes.c_char_p, []),
+    "msgb_version": (ctypes.c_char_p, []),
+    "msgb_sum_fwd_f64": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp]),
+    "msgb_adj_gather_f64": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "msgb_sum_f32_workspace_size": (c_sz, [c_vp, c_i64]),
+    "msgb_sum_fwd_f32": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_sz, c_vp, c_vp]),
+    "msgb_adj_gather_f32": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_sz, c_vp, c_vp, c_vp]),
+    "msgb_mswpt_create": (ctypes.c_int, [c_vp, c_vp]),
+    "msgb_mswpt_destroy": (ctypes.c_int, [c_vp]),
+    "msgb_mswpt_total_coeffs": (c_i64, [c_vp]),
+    "msgb_mswpt_workspace_size": (c_sz, [c_vp]),
+    "msgb_mswpt_forward": (ctypes.c_int, [c_vp, c_vp, ctypes.c_int, ctypes.c_int, c_dbl,
+                                           ctypes.c_int, c_vp, c_vp, c_vp, c_sz, c_vp]),
+    "msgb_mswpt_synthesis": (ctypes.c_int, [c_vp, c_vp, ctypes.c_int, ctypes.c_int, c_vp, c_vp,
+                                             c_sz, c_vp]),
+    "msgb_topn_workspace_size": (c_sz, [c_i64, c_i64]),
+    "msgb_topn": (ctypes.c_int, [c_vp, c_vp, c_i64, c_i64, c_vp, c_vp, c_vp, c_sz, c_vp]),
+    "msgb_beam_init": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_i64, c_vp, c_vp]),
+    "msgb_scatter_coeff_grad": (ctypes.c_int, [c_vp, c_vp, c_i64, c_dbl, c_vp, ctypes.c_int,
+                                                c_vp, c_vp]),
+}
+
+_lock = threading.Lock()
+_lib = None
+
+
+def lib():
+    """Load libmsgb.so once; raises RuntimeError when it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(
+                    f"libmsgb.so not found at {LIB_PATH}; build it with "
+                    "`python -m beamax_b200.build` (the CUDA path has no fallback)")
+            L = ctypes.CDLL(LIB_PATH)
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(L, name, None)
+                if fn is None:
+                    continue  # reported by missing_symbols(); calls raise AttributeError
+                fn.restype = res
+                fn.argtypes = args
+            _lib = L
+    return _lib
+
+
+def missing_symbols():
+    """Entry points of include/msgb.h that the loaded library does not export."""
+    L = lib()
+    return [n for n in SIGNATURES if getattr(L, n, None) is None]
+
+
+def last_error() -> str:
+    return lib().msgb_last_error().decode(errors="replace")
+
+
+def check(status: int, what: str) -> None:
+    if status != 0:
+        raise RuntimeError(f"{what} failed ({STATUS.get(status, status)}): {last_error()}")
+
+
+def ref(obj) -> int:
+    return ctypes.addressof(obj)

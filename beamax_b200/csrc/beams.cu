@@ -1,0 +1,258 @@
+// top_n selection, beam initialisation and the coefficient-space scatter of
+// the transpose.
+//
+// top_n restates forward_solver_utils.py:65-89 with jnp.argpartition's tie
+// rule: keys are the IEEE bit patterns of sqrt(re*re + im*im) (monotone for
+// non-negative doubles); a stable ascending radix sort of (key, index) pairs
+// orders them by (key, index) and the last n entries are the selection, in the
+// order the reference returns them (increasing magnitude, ties by index).
+//
+// Beam init restates compute_forward_parameters (forward_solver_utils.py:
+// 255-373), compute_frame_phase (transforms.py:193-226) and
+// _coefficient_positions (forward_solver_utils.py:233-252).
+#include <cub/cub.cuh>
+
+#include "common.cuh"
+
+// Layout shared with mswpt.cu (only the fields read here).
+struct msgb_mswpt;
+
+namespace msgb {
+struct PlanView {
+    int nd, red, levels;
+    int N[3], aspect[3];
+    int64_t ccum[9];
+    int bcum[9];
+    int bl[8];
+    int bshape[8][3];
+    const int32_t *centres;
+};
+int plan_view(const msgb_mswpt *p, PlanView &v);
+}  // namespace msgb
+
+namespace msgb {
+namespace {
+
+__global__ void key_bits_kernel(const double *keys, int64_t n, uint64_t *kb, int32_t *idx) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double k = keys[i];
+    if (k == 0.0) k = 0.0;  // fold -0.0 onto +0.0
+    kb[i] = (uint64_t)__double_as_longlong(k);
+    idx[i] = (int32_t)i;
+}
+
+__global__ void take_last_kernel(const int32_t *sorted_idx, int64_t total, int64_t n, const double2 *coeffs,
+                                 int64_t *idx_out, double2 *val_out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t j = sorted_idx[total - n + i];
+    idx_out[i] = j;
+    if (val_out) val_out[i] = coeffs[j];
+}
+
+__device__ __forceinline__ int floordiv(int a, int b) {
+    int q = a / b;
+    if ((a % b != 0) && ((a < 0) != (b < 0))) --q;
+    return q;
+}
+
+struct InitArgs {
+    PlanView v;
+    double L[3];
+    const int64_t *idx;
+    const double2 *values;
+    int64_t n;
+    msgb_beam_out out;
+};
+
+__global__ void beam_init_kernel(InitArgs A) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    const PlanView &v = A.v;
+    const int nd = v.nd;
+    const int64_t flat = A.idx[i];
+    // level = searchsorted(cumsum(prod shapes), flat, 'right')
+    int l = 0;
+    while (l < v.levels - 1 && flat >= v.ccum[l + 1]) ++l;
+    const int64_t local = flat - v.ccum[l];
+    int S[3] = {1, 1, 1};
+    int64_t P = 1;
+    for (int a = 0; a < nd; ++a) {
+        S[a] = 2 * v.bshape[l][a];
+        P *= S[a];
+    }
+    const int64_t box_local = local / P;
+    int64_t rem = local - box_local * P;
+    int k[3] = {0, 0, 0};
+    for (int a = nd - 1; a >= 0; --a) {
+        k[a] = (int)(rem % S[a]);
+        rem /= S[a];
+    }
+    const int64_t box = v.bcum[l] + box_local;
+    double cen[3], norm2 = 0.0;
+    int ci[3];
+    for (int a = 0; a < nd; ++a) {
+        ci[a] = v.centres[box * nd + a];
+        cen[a] = (double)ci[a] / A.L[a];
+        norm2 += cen[a] * cen[a];
+    }
+    const double norm = sqrt(norm2);
+    const double pi = 3.141592653589793;
+    double a0 = 1.0, cycles = 0.0;
+    for (int a = 0; a < nd; ++a) {
+        const double bl = (double)v.bl[l] / A.L[a] * (double)v.aspect[a];
+        const double Ll = bl * v.red;
+        const double sig = bl / 2.0;
+        const double ps = pi * sig;
+        A.out.p0[i * nd + a] = 2.0 * pi * cen[a] / norm;
+        A.out.alpha[2 * (i * nd + a)] = 0.0;
+        A.out.alpha[2 * (i * nd + a) + 1] = 2.0 * (ps * ps) / norm;
+        a0 *= sqrt((pi * A.L[a]) / (Ll * (double)v.N[a])) * sig;
+        // frame phase (transforms.py:207-226)
+        const int support = v.bl[l] * v.red * v.aspect[a];
+        const int half = support / 2;
+        const int parity = floordiv(ci[a] + v.N[a] / 2, half);
+        const int sign = 1 - 2 * (parity & 1);
+        const int rolls = sign * (half / 2);
+        cycles += (double)(ci[a] - rolls) * (double)k[a] / (double)support;
+        // _coefficient_positions (forward_solver_utils.py:233-252)
+        A.out.x0[i * nd + a] = (double)k[a] * A.L[a] / (double)support;
+    }
+    cycles = cycles - floor(cycles);  // jnp.remainder(., 1.0)
+    double s, c;
+    sincospi(2.0 * cycles, &s, &c);
+    cd au = cd{a0 * c, a0 * s};
+    if (A.out.a0_unit) {
+        A.out.a0_unit[2 * i] = au.re;
+        A.out.a0_unit[2 * i + 1] = au.im;
+    }
+    cd val = A.values ? cd{A.values[i].x, A.values[i].y} : cd{1.0, 0.0};
+    cd a = au * val;
+    A.out.a0[2 * i] = a.re;
+    A.out.a0[2 * i + 1] = a.im;
+    A.out.omega[i] = norm;
+}
+
+struct ScatterArgs {
+    const int64_t *idx;
+    const double2 *g;
+    int64_t n;
+    double scale;
+    int mask;
+    int levels;
+    int64_t ccum[9];
+    double2 *G;
+};
+
+__global__ void scatter_kernel(ScatterArgs A) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    const int64_t f = A.idx[i];
+    double m = A.scale;
+    if (A.mask) {
+        int l = 0;
+        while (l < A.levels - 1 && f >= A.ccum[l + 1]) ++l;
+        const int64_t seg = A.ccum[l + 1] - A.ccum[l];
+        if (f - A.ccum[l] >= seg / 2) m = 0.0;
+    }
+    const double2 v = A.g[i];
+    double2 o = A.G[f];
+    A.G[f] = make_double2(o.x + m * v.x, o.y + m * v.y);
+}
+
+size_t a256(size_t x) { return (x + 255) & ~size_t(255); }
+
+struct TopnLayout {
+    size_t kin, kout, vin, vout, cub, total, cub_bytes;
+};
+
+TopnLayout topn_layout(int64_t total) {
+    TopnLayout l{};
+    cub::DeviceRadixSort::SortPairs(nullptr, l.cub_bytes, (const uint64_t *)nullptr, (uint64_t *)nullptr,
+                                    (const int32_t *)nullptr, (int32_t *)nullptr, (int)total);
+    size_t o = 0;
+    l.kin = o; o = a256(o + 8 * total);
+    l.kout = o; o = a256(o + 8 * total);
+    l.vin = o; o = a256(o + 4 * total);
+    l.vout = o; o = a256(o + 4 * total);
+    l.cub = o; o = a256(o + l.cub_bytes);
+    l.total = o;
+    return l;
+}
+
+}  // namespace
+}  // namespace msgb
+
+using namespace msgb;
+
+extern "C" size_t msgb_topn_workspace_size(int64_t total, int64_t n) {
+    (void)n;
+    if (total <= 0 || total > 0x7fffffffLL) return 0;
+    return topn_layout(total).total;
+}
+
+extern "C" int msgb_topn(const double *keys, const double *coeffs, int64_t total, int64_t n, int64_t *idx,
+                         double *values, void *workspace, size_t workspace_bytes, msgb_stream_t stream) {
+    if (!keys || !idx) return fail(MSGB_ERR_ARG, "msgb_topn: NULL keys or idx");
+    if (values && !coeffs) return fail(MSGB_ERR_ARG, "msgb_topn: values requested without coeffs");
+    if (total <= 0 || total > 0x7fffffffLL) return fail(MSGB_ERR_UNSUPPORTED, "msgb_topn: total out of range");
+    if (n <= 0) return fail(MSGB_ERR_ARG, "top_n threshold must be a positive integer.");
+    if (n > total) n = total;
+    const TopnLayout l = topn_layout(total);
+    if (!workspace || workspace_bytes < l.total)
+        return fail(MSGB_ERR_WORKSPACE, "msgb_topn: workspace too small: need %zu, got %zu", l.total, workspace_bytes);
+    if (((uintptr_t)workspace & 255) != 0) return fail(MSGB_ERR_WORKSPACE, "workspace must be 256-byte aligned");
+    cudaStream_t st = as_stream(stream);
+    char *ws = (char *)workspace;
+    uint64_t *kin = (uint64_t *)(ws + l.kin), *kout = (uint64_t *)(ws + l.kout);
+    int32_t *vin = (int32_t *)(ws + l.vin), *vout = (int32_t *)(ws + l.vout);
+    const unsigned blocks = (unsigned)((total + 255) / 256);
+    key_bits_kernel<<<blocks, 256, 0, st>>>(keys, total, kin, vin);
+    size_t cb = l.cub_bytes;
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(ws + l.cub, cb, kin, kout, vin, vout, (int)total, 0, 64, st);
+    if (e != cudaSuccess) return fail(MSGB_ERR_CUDA, "msgb_topn sort: %s", cudaGetErrorString(e));
+    take_last_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(vout, total, n, (const double2 *)coeffs, idx,
+                                                                 (double2 *)values);
+    return check_launch("msgb_topn");
+}
+
+extern "C" int msgb_beam_init(const msgb_mswpt *plan, const double *L, const int64_t *idx, const double *values,
+                              int64_t n, const msgb_beam_out *out, msgb_stream_t stream) {
+    if (!plan || !L || !out) return fail(MSGB_ERR_ARG, "msgb_beam_init: NULL argument");
+    if (n == 0) return MSGB_OK;
+    if (!idx || !out->x0 || !out->p0 || !out->alpha || !out->a0 || !out->omega)
+        return fail(MSGB_ERR_ARG, "msgb_beam_init: NULL array");
+    InitArgs A{};
+    if (int e = plan_view(plan, A.v)) return e;
+    for (int a = 0; a < 3; ++a) A.L[a] = a < A.v.nd ? L[a] : 1.0;
+    A.idx = idx;
+    A.values = (const double2 *)values;
+    A.n = n;
+    A.out = *out;
+    beam_init_kernel<<<(unsigned)((n + 255) / 256), 256, 0, as_stream(stream)>>>(A);
+    return check_launch("msgb_beam_init");
+}
+
+extern "C" int msgb_scatter_coeff_grad(const int64_t *idx, const double *g, int64_t n, double scale,
+                                       const msgb_mswpt *plan, int apply_half_mask, double *G,
+                                       msgb_stream_t stream) {
+    if (!idx || !g || !G) return fail(MSGB_ERR_ARG, "msgb_scatter_coeff_grad: NULL argument");
+    if (n == 0) return MSGB_OK;
+    ScatterArgs A{};
+    A.idx = idx;
+    A.g = (const double2 *)g;
+    A.n = n;
+    A.scale = scale;
+    A.mask = apply_half_mask;
+    A.G = (double2 *)G;
+    if (apply_half_mask) {
+        if (!plan) return fail(MSGB_ERR_ARG, "msgb_scatter_coeff_grad: half mask needs the plan");
+        PlanView v;
+        if (int e = plan_view(plan, v)) return e;
+        A.levels = v.levels;
+        for (int l = 0; l <= v.levels; ++l) A.ccum[l] = v.ccum[l];
+    }
+    scatter_kernel<<<(unsigned)((n + 255) / 256), 256, 0, as_stream(stream)>>>(A);
+    return check_launch("msgb_scatter_coeff_grad");
+}

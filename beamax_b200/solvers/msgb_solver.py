@@ -1,0 +1,418 @@
+"""``MSGBSolver``: MSGB forward operator and its exact transpose on a B200.
+
+Drop-in for beamax's ``MSGBSolver`` (solvers/msgb_solvers/msgb_solver.py:
+358-1386) on the forward path.  ``forward(p0, domain, sensors, ts, wpt)``
+runs, all on the GPU through libmsgb.so:
+
+1. ``msgb_mswpt_forward``  - coefficients c_pos = 0.5 * MSWPT(p0) * half_mask
+   (compute_coefficients, forward_solver_utils.py:716-786) plus top_n keys;
+2. ``msgb_topn``           - the ``thr`` largest, ties by index (:65-89);
+3. ``msgb_beam_init``      - beam data (compute_forward_parameters, :255-373);
+4. ``msgb_sum_fwd_f64`` (dense, reference semantics) or ``msgb_sum_fwd_f32``
+   (Gaussian cutoff, Kahan sums) - both branches (modes +1/-1) of every beam
+   with solve_hom_diag fused in (gb/core.py:194-329).
+
+``adjoint(data, domain, sensors, ts, wpt)`` is the exact transpose of that
+map with the beam selection frozen (the reference's jax.vjp pattern,
+examples/diagnostics/msgb_adjoint_pairing.py:156-165): per-beam gathers
+(``msgb_adj_gather_*``), a scatter to coefficient space and the Hermitian
+adjoint of the MSWPT.  The reference's own principal-symbol ``adjoint`` (seven
+arguments, msgb_solver.py:1235-1386) is a different operator and raises
+``NotImplementedError`` here.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass
+from numbers import Integral, Real
+from typing import Optional, Tuple
+
+import numpy as np
+
+from .. import _lib
+from .._device import DeviceCache, as_device_f64, default_device, workspace
+from ..geometry import Domain, Sensor
+from ..gb.gb_solvers import solver_name
+from ..transforms import MSWPT
+
+_cache = DeviceCache()
+
+
+def _validate_time_grid(ts, *, allow_singleton: bool = False) -> Optional[float]:
+    """msgb_solver.py:41-65."""
+    ts_np = np.asarray(ts.detach().cpu().numpy() if hasattr(ts, "detach") else ts)
+    if ts_np.ndim != 1 or ts_np.size == 0:
+        raise ValueError("ts must be a non-empty one-dimensional array.")
+    if not np.all(np.isfinite(ts_np)):
+        raise ValueError("ts must contain only finite values.")
+    if ts_np.size == 1:
+        if allow_singleton:
+            return None
+        raise ValueError("ts must be one-dimensional with at least two points.")
+    diffs = np.diff(ts_np)
+    if np.any(diffs <= 0) or not np.allclose(diffs, diffs[0], rtol=1e-6, atol=0.0):
+        raise ValueError("ts must be finite, strictly increasing, and uniformly spaced.")
+    return float(diffs[0])
+
+
+@dataclass
+class Selection:
+    """Frozen beam selection: flat coefficient indices and their c_pos values (device)."""
+
+    idx: "object"      # (n,) int64 CUDA tensor
+    values: "object"   # (n,) complex128 CUDA tensor
+    total_coeffs: int
+
+
+@dataclass
+class BeamTensors:
+    x0: "object"
+    p0: "object"
+    alpha: "object"    # complex128 (n, d)
+    a0: "object"       # complex128 (n,)
+    a0_unit: "object"  # complex128 (n,)
+    omega: "object"
+
+    @property
+    def n(self) -> int:
+        return int(self.omega.shape[0])
+
+    def beam_set(self, unit: bool = False) -> _lib.BeamSet:
+        import torch
+
+        a0 = self.a0_unit if unit else self.a0
+        return _lib.BeamSet(n=self.n, x0=self.x0.data_ptr(), p0=self.p0.data_ptr(),
+                            alpha=torch.view_as_real(self.alpha).data_ptr(),
+                            a0=torch.view_as_real(a0).data_ptr(), omega=self.omega.data_ptr())
+
+
+class MSGBSolver:
+    """Multiscale Gaussian beam solver (msgb_solver.py:358-534 options and checks).
+
+    Extra keyword-only options (no reference counterpart):
+      precision: "fp64" (dense, reference semantics) or "fp32" (FP32
+        evaluation, Kahan-compensated sums, FP64 anchor phases, Gaussian cutoff).
+      cutoff: e-folds of the Gaussian envelope beyond which the FP32 path skips
+        a (beam, time tile, sensor tile) triple.
+    """
+
+    def __init__(self, thr, thr_strat: str, batch_size: int, input_type: str, ode_solver, sum_method: str,
+                 tr_ode_solver=None, sharding=None, ode_config=None, adjoint_relative_guard: float = 5e-2,
+                 *, precision: str = "fp64", cutoff: float = 16.0):
+        valid_thresholds = {"hard", "top_n", "percentile", "hard_reassign", "bao_energy", "perc_max_abs"}
+        if thr_strat not in valid_thresholds:
+            raise ValueError(f"thr_strat must be one of {', '.join(sorted(valid_thresholds))}; got {thr_strat!r}.")
+        if isinstance(thr, bool) or not isinstance(thr, Real):
+            raise ValueError(f"thr must be a finite real scalar; got {thr!r}.")
+        if not math.isfinite(float(thr)):
+            raise ValueError(f"thr must be finite; got {thr!r}.")
+        if thr_strat == "top_n":
+            if not isinstance(thr, Integral) or int(thr) <= 0:
+                raise ValueError("top_n threshold must be a positive integer.")
+            thr = int(thr)
+        elif thr_strat == "percentile":
+            if not 0 <= float(thr) <= 100:
+                raise ValueError("percentile threshold must lie in [0, 100].")
+            thr = float(thr)
+        elif thr_strat in {"hard_reassign", "perc_max_abs"}:
+            if not 0 <= float(thr) <= 1:
+                raise ValueError(f"{thr_strat} threshold must lie in [0, 1].")
+            thr = float(thr)
+        else:
+            if float(thr) < 0:
+                raise ValueError(f"{thr_strat} threshold must be non-negative.")
+            thr = float(thr)
+        if input_type not in {"spatial", "fourier"}:
+            raise ValueError(f"input_type must be 'spatial' or 'fourier'; got {input_type!r}.")
+        if batch_size <= 0:
+            raise ValueError(f"batch_size must be positive; got {batch_size}.")
+        if not 0.0 <= adjoint_relative_guard < 1.0:
+            raise ValueError(f"adjoint_relative_guard must lie in [0, 1); got {adjoint_relative_guard}.")
+        valid_sum = {"all_real", "scan_real", "vmap_real", "all_complex", "scan_complex", "vmap_complex"}
+        if sum_method not in valid_sum:
+            raise ValueError(f"sum_method must be one of {', '.join(sorted(valid_sum))}; got {sum_method!r}.")
+        if precision not in ("fp64", "fp32"):
+            raise ValueError(f"precision must be 'fp64' or 'fp32'; got {precision!r}.")
+        self.thr = thr
+        self.thr_strat = thr_strat
+        self.batch_size = batch_size
+        self.input_type = input_type
+        self.ode_solver = ode_solver
+        self.ode_solver_name = solver_name(ode_solver)
+        self.tr_ode_solver = ode_solver if tr_ode_solver is None else tr_ode_solver
+        self.sharding = sharding
+        self.ode_config = ode_config
+        self.adjoint_relative_guard = float(adjoint_relative_guard)
+        self.use_real = "real" in sum_method
+        self.aggregate_method = "scan" if "scan" in sum_method else ("vmap" if "vmap" in sum_method else "all")
+        self.sum_method = sum_method
+        self.precision = precision
+        self.cutoff = float(cutoff)
+        self.last_selection: Optional[Selection] = None
+        self.last_eval_count: Optional[int] = None
+
+    # ------------------------------------------------------------- helpers
+    def _effective_top_n(self, wpt: MSWPT, *, half_frame: bool = False):
+        """msgb_solver.py:536-549."""
+        if self.thr_strat != "top_n":
+            return self.thr
+        cap = wpt.half_frame_capacity() if half_frame else wpt.total_coeffs
+        return min(int(self.thr), int(cap))
+
+    @staticmethod
+    def _sensor_positions(sensors) -> np.ndarray:
+        if isinstance(sensors, Sensor):
+            return sensors.positions
+        if hasattr(sensors, "detach"):
+            return sensors.detach().cpu().numpy()
+        if isinstance(sensors, np.ndarray):
+            return sensors
+        raise ValueError("Unsupported sensor type")
+
+    def _problem(self, domain: Domain, sensors, ts, device):
+        import torch
+
+        c = domain.constant_speed()
+        if c is None:
+            raise NotImplementedError("heterogeneous sound speed needs the RK4 beam path")
+        if domain.lam != 0.0:
+            raise NotImplementedError("absorption (lam != 0) is not supported by the summation kernels")
+        pos = np.ascontiguousarray(self._sensor_positions(sensors), np.float64)
+        if pos.ndim != 2 or pos.shape[1] != domain.ndim:
+            raise ValueError(f"sensor positions must have shape (Ns, {domain.ndim})")
+        ts_np = np.ascontiguousarray(ts.detach().cpu().numpy() if hasattr(ts, "detach") else np.asarray(ts),
+                                     np.float64)
+        ts_d = torch.from_numpy(ts_np).to(device)
+        sens_key = sensors if isinstance(sensors, Sensor) else None
+        if sens_key is not None:
+            sd = _cache.get(sens_key, ("pos", str(device)), lambda: torch.from_numpy(pos).to(device))
+        else:
+            sd = torch.from_numpy(pos).to(device)
+        L = domain.grid_size
+        pr = _lib.Problem()
+        pr.ndim = domain.ndim
+        for a in range(3):
+            pr.periodic[a] = int(domain.periodic[a]) if a < domain.ndim else 0
+            pr.L[a] = float(L[a]) if a < domain.ndim else 1.0
+        pr.c = float(c)
+        pr.nt = ts_np.size
+        pr.ts = ts_d.data_ptr()
+        pr.ns = pos.shape[0]
+        pr.sensors = sd.data_ptr()
+        return pr, (ts_d, sd)
+
+    # ------------------------------------------------------------- pipeline
+    def select(self, p0, domain: Domain, wpt: MSWPT, dpdt=None) -> Selection:
+        """c_pos on the GPU, then top_n (msgb_solver.py:570-612)."""
+        import torch
+
+        if self.thr_strat != "top_n":
+            raise NotImplementedError(f"thr_strat={self.thr_strat!r}: only top_n runs on the GPU path")
+        x = as_device_f64(p0)
+        if x.is_complex():
+            raise NotImplementedError("complex p0 (the *_complex parameter path) is not implemented")
+        if dpdt is not None:
+            dz = dpdt.detach() if hasattr(dpdt, "detach") else np.asarray(dpdt)
+            nonzero = bool((dz != 0).any()) if hasattr(dz, "any") else bool(np.any(dz))
+            if nonzero:
+                raise NotImplementedError("non-zero dpdt is not implemented on the GPU path")
+        coeffs, keys = wpt.forward_device(x, self.input_type, scale=0.5, half_mask=True, keys=True)
+        n = self._effective_top_n(wpt, half_frame=True)
+        dev = x.device
+        idx = torch.empty(n, dtype=torch.int64, device=dev)
+        vals = torch.empty(n, dtype=torch.complex128, device=dev)
+        nbytes = _lib.lib().msgb_topn_workspace_size(wpt.total_coeffs, n)
+        ws = workspace(dev, "topn", nbytes)
+        st = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(_lib.lib().msgb_topn(keys.data_ptr(), torch.view_as_real(coeffs).data_ptr(), wpt.total_coeffs,
+                                        n, idx.data_ptr(), torch.view_as_real(vals).data_ptr(), ws.data_ptr(),
+                                        nbytes, st), "msgb_topn")
+        return Selection(idx, vals, wpt.total_coeffs)
+
+    def beams(self, sel: Selection, domain: Domain, wpt: MSWPT) -> BeamTensors:
+        """Beam data for a selection (compute_forward_parameters, a0 *= coefficient)."""
+        import torch
+
+        dev = sel.idx.device
+        n = int(sel.idx.shape[0])
+        d = domain.ndim
+        x0 = torch.empty((n, d), dtype=torch.float64, device=dev)
+        p0 = torch.empty((n, d), dtype=torch.float64, device=dev)
+        al = torch.empty((n, d), dtype=torch.complex128, device=dev)
+        a0 = torch.empty(n, dtype=torch.complex128, device=dev)
+        a0u = torch.empty(n, dtype=torch.complex128, device=dev)
+        om = torch.empty(n, dtype=torch.float64, device=dev)
+        out = _lib.BeamOut(x0=x0.data_ptr(), p0=p0.data_ptr(), alpha=torch.view_as_real(al).data_ptr(),
+                           a0=torch.view_as_real(a0).data_ptr(), omega=om.data_ptr(),
+                           a0_unit=torch.view_as_real(a0u).data_ptr())
+        L = (ctypes.c_double * 3)(*[float(v) for v in domain.grid_size], *([1.0] * (3 - d)))
+        st = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(_lib.lib().msgb_beam_init(wpt.plan(dev), L, sel.idx.data_ptr(),
+                                             torch.view_as_real(sel.values).data_ptr(), n, _lib.ref(out), st),
+                   "msgb_beam_init")
+        return BeamTensors(x0, p0, al, a0, a0u, om)
+
+    def sum_forward(self, bt: BeamTensors, domain: Domain, sensors, ts):
+        """Beam summation at the sensors: (Nt, Ns) float64 (fp64) or float32 (fp32)."""
+        import torch
+
+        dev = bt.x0.device
+        pr, keep = self._problem(domain, sensors, ts, dev)
+        bs = bt.beam_set(unit=False)
+        st = torch.cuda.current_stream(dev).cuda_stream
+        if self.precision == "fp64":
+            out = torch.empty((pr.nt, pr.ns), dtype=torch.float64, device=dev)
+            _lib.check(_lib.lib().msgb_sum_fwd_f64(_lib.ref(pr), _lib.ref(bs), out.data_ptr(), st),
+                       "msgb_sum_fwd_f64")
+            return out
+        out = torch.empty((pr.nt, pr.ns), dtype=torch.float32, device=dev)
+        cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+        opts = _lib.SumOpts(cutoff=self.cutoff, eval_count=cnt.data_ptr())
+        nbytes = _lib.lib().msgb_sum_f32_workspace_size(_lib.ref(pr), bt.n)
+        ws = workspace(dev, "sum32", nbytes)
+        _lib.check(_lib.lib().msgb_sum_fwd_f32(_lib.ref(pr), _lib.ref(bs), _lib.ref(opts), ws.data_ptr(), nbytes,
+                                               out.data_ptr(), st), "msgb_sum_fwd_f32")
+        self._eval_counter = cnt
+        return out
+
+    def gather_adjoint(self, bt: BeamTensors, domain: Domain, sensors, ts, data):
+        """Per selected coefficient g_j = sum 2 d conj(K_j) over both modes: (n,) complex128."""
+        import torch
+
+        dev = bt.x0.device
+        pr, keep = self._problem(domain, sensors, ts, dev)
+        bs = bt.beam_set(unit=True)
+        g = torch.empty(bt.n, dtype=torch.complex128, device=dev)
+        st = torch.cuda.current_stream(dev).cuda_stream
+        if self.precision == "fp64":
+            d = as_device_f64(data, dev).reshape(pr.nt, pr.ns).contiguous()
+            _lib.check(_lib.lib().msgb_adj_gather_f64(_lib.ref(pr), _lib.ref(bs), d.data_ptr(),
+                                                      torch.view_as_real(g).data_ptr(), st), "msgb_adj_gather_f64")
+            return g
+        d = as_device_f64(data, dev).to(torch.float32).reshape(pr.nt, pr.ns).contiguous()
+        cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+        opts = _lib.SumOpts(cutoff=self.cutoff, eval_count=cnt.data_ptr())
+        nbytes = _lib.lib().msgb_sum_f32_workspace_size(_lib.ref(pr), bt.n)
+        ws = workspace(dev, "sum32", nbytes)
+        _lib.check(_lib.lib().msgb_adj_gather_f32(_lib.ref(pr), _lib.ref(bs), _lib.ref(opts), ws.data_ptr(), nbytes,
+                                                  d.data_ptr(), torch.view_as_real(g).data_ptr(), st),
+                   "msgb_adj_gather_f32")
+        self._eval_counter = cnt
+        return g
+
+    def coefficient_adjoint(self, sel: Selection, g, wpt: MSWPT):
+        """Transpose of c_pos[idx] -> image: scatter 0.5 * g (half mask), MSWPT^H, real part."""
+        import torch
+
+        dev = g.device
+        G = torch.zeros(wpt.total_coeffs, dtype=torch.complex128, device=dev)
+        st = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(_lib.lib().msgb_scatter_coeff_grad(sel.idx.data_ptr(), torch.view_as_real(g).data_ptr(),
+                                                      int(sel.idx.shape[0]), 0.5, wpt.plan(dev), 1,
+                                                      torch.view_as_real(G).data_ptr(), st),
+                   "msgb_scatter_coeff_grad")
+        return wpt.adjoint(G, "spatial", real_output=True)
+
+    # ------------------------------------------------------------- public API
+    def _check_forward_args(self, p0, domain: Domain, ts, wpt: MSWPT, dpdt):
+        shape = tuple(p0.shape)
+        if shape != domain.N or (dpdt is not None and tuple(dpdt.shape) != domain.N):
+            raise ValueError(f"p0 and dpdt must both have shape {domain.N}; got {shape} and "
+                             f"{tuple(dpdt.shape) if dpdt is not None else shape}.")
+        if wpt.dyadic_decomp.N != domain.N:
+            raise ValueError("wpt grid shape must match domain.N.")
+        _validate_time_grid(ts, allow_singleton=True)
+        if not self.use_real:
+            raise NotImplementedError(f"sum_method={self.sum_method!r}: complex summation is not implemented")
+
+    def forward(self, p0, domain: Domain, sensors, ts, wpt: MSWPT, *, dpdt=None):
+        """Pressure at the sensors, shape (Nt, Ns) (msgb_solver.py:858-899)."""
+        data, _ = self._forward_impl(p0, domain, sensors, ts, wpt, dpdt, want_params=False)
+        return data
+
+    def forward_with_params(self, p0, domain: Domain, sensors, ts, wpt: MSWPT, *, dpdt=None):
+        """Sensor data and the beam parameters (p0s, M0s, x0s, omegas, a0s, modes)
+        (msgb_solver.py:901-982), mirrored over the two modes and batched as the
+        reference does for scan/vmap aggregation (coeff_index.py:29-87)."""
+        return self._forward_impl(p0, domain, sensors, ts, wpt, dpdt, want_params=True)
+
+    def _forward_impl(self, p0, domain, sensors, ts, wpt, dpdt, want_params):
+        self._check_forward_args(p0, domain, ts, wpt, dpdt)
+        self._sensor_positions(sensors)
+        sel = self.select(p0, domain, wpt, dpdt)
+        bt = self.beams(sel, domain, wpt)
+        out = self.sum_forward(bt, domain, sensors, ts)
+        self.last_selection = sel
+        result = out if _is_torch(p0) else out.cpu().numpy()
+        if not want_params:
+            return result, None
+        return result, self._params_like_reference(bt, domain, as_numpy=not _is_torch(p0))
+
+    def _params_like_reference(self, bt: BeamTensors, domain: Domain, as_numpy: bool):
+        import torch
+
+        d = domain.ndim
+        eye = torch.eye(d, dtype=torch.complex128, device=bt.alpha.device)
+        M0 = bt.alpha[:, :, None] * eye
+        cat = lambda t: torch.cat([t, t], 0)
+        n = bt.n
+        modes = torch.cat([torch.ones(n, dtype=torch.float64, device=bt.omega.device),
+                           -torch.ones(n, dtype=torch.float64, device=bt.omega.device)])
+        params = [cat(bt.p0), cat(M0), cat(bt.x0), cat(bt.omega), cat(bt.a0), modes]
+        if self.aggregate_method in ("scan", "vmap"):
+            b = params[0].shape[0]
+            nb = (b + self.batch_size - 1) // self.batch_size
+            pad = nb * self.batch_size - b
+            out = []
+            for i, t in enumerate(params):
+                if pad:
+                    filler = torch.zeros((pad,) + t.shape[1:], dtype=t.dtype, device=t.device) if i == 4 \
+                        else t[-1:].expand((pad,) + t.shape[1:])
+                    t = torch.cat([t, filler], 0)
+                out.append(t.reshape((nb, self.batch_size) + t.shape[1:]))
+            params = out
+        if as_numpy:
+            params = [p.cpu().numpy() for p in params]
+        return tuple(params)
+
+    def adjoint(self, data, domain: Domain, sensors, ts, wpt: MSWPT, *args, p0=None,
+                selection: Optional[Selection] = None, **kwargs):
+        """Exact transpose A^T d of ``forward`` with the beam selection frozen.
+
+        The selection is ``selection`` if given, else the one made from ``p0``,
+        else the one made by this solver's last ``forward``.  Returns the image
+        (shape domain.N), float64.  The reference's seven-argument
+        principal-symbol adjoint is not this operator.
+        """
+        if args or {"sources", "data_domain", "data_wpt", "window"} & set(kwargs):
+            raise NotImplementedError(
+                "the principal-symbol adjoint adjoint(data, domain, sensors, sources, ts, data_domain, "
+                "data_wpt) is not implemented; adjoint(data, domain, sensors, ts, wpt) is the exact "
+                "transpose of forward")
+        if kwargs:
+            raise TypeError(f"unexpected keyword arguments {sorted(kwargs)}")
+        if wpt.dyadic_decomp.N != domain.N:
+            raise ValueError("wpt grid shape must match domain.N.")
+        _validate_time_grid(ts, allow_singleton=True)
+        if selection is None:
+            if p0 is not None:
+                selection = self.select(p0, domain, wpt)
+            elif self.last_selection is not None and self.last_selection.total_coeffs == wpt.total_coeffs:
+                selection = self.last_selection
+            else:
+                raise ValueError("adjoint needs a beam selection: call forward first or pass p0= or selection=")
+        bt = self.beams(selection, domain, wpt)
+        g = self.gather_adjoint(bt, domain, sensors, ts, data)
+        img = self.coefficient_adjoint(selection, g, wpt)
+        return img if _is_torch(data) else img.cpu().numpy()
+
+    def eval_count(self) -> Optional[int]:
+        """Evaluated (beam, time, sensor) triples of the last FP32 call."""
+        c = getattr(self, "_eval_counter", None)
+        return None if c is None else int(c.item())
+
+
+def _is_torch(x) -> bool:
+    return hasattr(x, "detach") and hasattr(x, "device")

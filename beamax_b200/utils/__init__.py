@@ -1,0 +1,3 @@
+"""Host helpers with the reference's names (beamax utils/)."""
+from .coeff_index import batch_data, compute_coeff_shapes, find_level, find_tensor_and_multiindex  # noqa: F401
+from .arrays import extract_centered_box, rel_l2  # noqa: F401

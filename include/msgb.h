@@ -1,0 +1,201 @@
+/*
+ * msgb.h - C ABI of libmsgb.so, the B200 (sm_100a) implementation of the
+ * multiscale Gaussian beam (MSGB) forward operator and its exact transpose.
+ *
+ * Every entry point works on caller-owned device memory, is ordered on the
+ * given CUDA stream, does not synchronise the host, and returns an int status
+ * (MSGB_OK = 0).  msgb_last_error() returns a thread-local message for the
+ * last failing call.  Entry points that need scratch memory take
+ * (void* workspace, size_t workspace_bytes) and have a *_workspace_size query;
+ * they never allocate.  Only msgb_mswpt_create allocates (the per-transform
+ * device tables, once), and msgb_mswpt_destroy frees them.
+ *
+ * Reference interfaces replaced (paths relative to the beamax project root):
+ *   MSWPT.forward / _compute_coeffs       beamax/transforms.py:591-733
+ *   MSWPT.inverse                          beamax/transforms.py:735-850
+ *   compute_coefficients (pos_only)        beamax/solvers/msgb_solvers/forward_solver_utils.py:716-786
+ *   _threshold_top_n                       beamax/solvers/msgb_solvers/forward_solver_utils.py:65-89
+ *   compute_forward_parameters             beamax/solvers/msgb_solvers/forward_solver_utils.py:255-373
+ *   solve_hom_diag                         beamax/gb/gb_solvers.py:356-422
+ *   compute_gaussian_beam_real (scan_real) beamax/gb/core.py:194-329
+ *   compute_forward_result                 beamax/solvers/msgb_solvers/forward_solver_utils.py:652-713
+ * The transpose entry points (msgb_adj_*, msgb_mswpt_adjoint) replace the
+ * reference's jax.vjp of the forward (examples/diagnostics/msgb_adjoint_pairing.py:156-165).
+ */
+#ifndef MSGB_H
+#define MSGB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *msgb_stream_t; /* == cudaStream_t */
+
+enum {
+    MSGB_OK = 0,
+    MSGB_ERR_ARG = 1,        /* invalid argument or shape */
+    MSGB_ERR_WORKSPACE = 2,  /* workspace missing or too small */
+    MSGB_ERR_CUDA = 3,       /* CUDA runtime / launch error */
+    MSGB_ERR_UNSUPPORTED = 4,/* configuration outside what the kernels support */
+    MSGB_ERR_NONFINITE = 5,  /* non-finite input detected */
+    MSGB_ERR_TIMEOUT = 6     /* a bounded device wait ran out */
+};
+
+/* Domain, medium and acquisition grid (device pointers for ts / sensors). */
+typedef struct msgb_problem {
+    int32_t ndim;            /* 1, 2 or 3 */
+    int32_t periodic[3];     /* per-axis periodic flags (geometry.py:25) */
+    double L[3];             /* physical size per axis, N * dx (geometry.py:226-236) */
+    double c;                /* constant sound speed (homogeneous entry points) */
+    int64_t nt;              /* number of time samples */
+    const double *ts;        /* (nt) */
+    int64_t ns;              /* number of sensors */
+    const double *sensors;   /* (ns, ndim), in the caller's order */
+} msgb_problem;
+
+/* Selected coefficients' beam data, positive branch (device, SoA).  Every
+ * coefficient is propagated twice, with mode +1 and mode -1
+ * (msgb_solver.py:612-619), so 2n beams are summed. */
+typedef struct msgb_beam_set {
+    int64_t n;
+    const double *x0;        /* (n, ndim) initial centres */
+    const double *p0;        /* (n, ndim) initial momenta, |p0| = 2 pi */
+    const double *alpha;     /* (n, ndim) complex (re, im): diagonal of M0 */
+    const double *a0;        /* (n) complex: amplitude; includes the coefficient for
+                                the forward, the unit amplitude for the adjoint */
+    const double *omega;     /* (n) frequency |xi| */
+} msgb_beam_set;
+
+/* Options of the FP32 summation. */
+typedef struct msgb_sum_opts {
+    double cutoff;           /* skip a (beam, tile) pair when the Gaussian exponent
+                                is provably above this many e-folds (<= 0: dense) */
+    unsigned long long *eval_count; /* optional device counter: evaluated
+                                (beam, t, sensor) triples are added to it */
+} msgb_sum_opts;
+
+const char *msgb_last_error(void);
+const char *msgb_version(void);
+
+/* ---- Gaussian-beam summation: replaces compute_gaussian_beam_real with
+ *      solve_hom_diag (gb/core.py:194-329, gb/gb_solvers.py:356-422) -------- */
+
+/* Dense FP64 forward, reference semantics (no cutoff).
+ * out: (nt, ns) FP64, overwritten. */
+int msgb_sum_fwd_f64(const msgb_problem *prob, const msgb_beam_set *beams, double *out,
+                     msgb_stream_t stream);
+
+/* Exact transpose of msgb_sum_fwd_f64 down to the coefficients:
+ * g[j] = sum_{mode, t, s} 2 data(t, s) conj(K_j(t, s)), contribution = 2 Re[c_j K_j].
+ * beams->a0 must hold the unit amplitude.  data: (nt, ns) FP64.  g: (n) complex. */
+int msgb_adj_gather_f64(const msgb_problem *prob, const msgb_beam_set *beams,
+                        const double *data, double *g, msgb_stream_t stream);
+
+/* FP32 forward with Kahan-compensated accumulation across beams, per-(beam,
+ * time) FP64 range-reduced anchor phases and Gaussian cutoff culling.
+ * out: (nt, ns) FP32.  The workspace (for n selected coefficients) covers
+ * both this call and msgb_adj_gather_f32. */
+size_t msgb_sum_f32_workspace_size(const msgb_problem *prob, int64_t n);
+int msgb_sum_fwd_f32(const msgb_problem *prob, const msgb_beam_set *beams,
+                     const msgb_sum_opts *opts, void *workspace, size_t workspace_bytes,
+                     float *out, msgb_stream_t stream);
+
+/* FP32 transpose of msgb_sum_fwd_f32 (same culling); one owner per beam, no
+ * atomics.  data: (nt, ns) FP32.  g: (n) complex FP64. */
+int msgb_adj_gather_f32(const msgb_problem *prob, const msgb_beam_set *beams,
+                        const msgb_sum_opts *opts, void *workspace, size_t workspace_bytes,
+                        const float *data, double *g, msgb_stream_t stream);
+
+/* ---- MSWPT tiling (transforms.py:357-850) ------------------------------ */
+
+typedef struct msgb_mswpt msgb_mswpt;
+
+/* Host-side description of a transform (all pointers are host memory). */
+typedef struct msgb_mswpt_desc {
+    int32_t ndim;
+    int32_t N[3];
+    int32_t aspect[3];           /* box_aspect_ratio */
+    int32_t redundancy;          /* 1 or 2 */
+    int32_t num_levels;
+    int32_t total_boxes;
+    const int32_t *box_length;   /* (num_levels) box_lengths (smallest axis) */
+    const int32_t *box_level;    /* (total_boxes) level of every box */
+    const int32_t *centres;      /* (total_boxes, ndim) centres_ndim */
+    const int32_t *box_shape;    /* (num_levels, ndim) half supports (box_shapes) */
+    const int64_t *coeffs_cumsum;/* (num_levels + 1) */
+    const int32_t *boxes_cumsum; /* (num_levels + 1) */
+    const double *gfilt;         /* concatenated per-level packed g, C order */
+    const int64_t *gfilt_offset; /* (num_levels) offsets into gfilt */
+    const double *sum_gsquare;   /* (prod N) */
+    /* lattice lookup used by the deterministic synthesis gather:
+     * per level, outer box counts per axis and a table mapping the lattice
+     * multi-index (C order) to the global box id or -1 (cut out). */
+    const int32_t *lattice_counts;  /* (num_levels, ndim) */
+    const int32_t *lattice_first;   /* (num_levels, ndim) first lattice centre per axis */
+    const int32_t *lattice_step;    /* (num_levels, ndim) lattice step per axis */
+    const int64_t *lattice_offset;  /* (num_levels) offsets into lattice_box */
+    const int32_t *lattice_box;     /* concatenated tables */
+} msgb_mswpt_desc;
+
+int msgb_mswpt_create(const msgb_mswpt_desc *desc, msgb_mswpt **plan);
+int msgb_mswpt_destroy(msgb_mswpt *plan);
+int64_t msgb_mswpt_total_coeffs(const msgb_mswpt *plan);
+size_t msgb_mswpt_workspace_size(const msgb_mswpt *plan);
+
+/* Analysis: coeffs = scale * MSWPT.forward(in) [* half_mask].
+ * in: prod(N) values, FP64, real (is_complex = 0) or interleaved complex.
+ * coeffs: (total_coeffs) complex FP64.  With keys != NULL also writes the
+ * top_n selection key sqrt(re*re + im*im) of every output coefficient. */
+int msgb_mswpt_forward(const msgb_mswpt *plan, const double *in, int is_complex,
+                       int input_is_fourier, double scale, int apply_half_mask,
+                       double *coeffs, double *keys, void *workspace, size_t workspace_bytes,
+                       msgb_stream_t stream);
+
+/* Synthesis.  mode bit 0 clear: MSWPT.inverse (transforms.py:735-850); set:
+ * the Hermitian adjoint of msgb_mswpt_forward (spatial input).  mode bit 1
+ * set: return the (shifted, unitary) Fourier-domain field instead of the
+ * spatial one.  out: prod(N) values, FP64; the real part only when
+ * real_output != 0, else interleaved complex.  The coefficient buffer is
+ * not modified. */
+int msgb_mswpt_synthesis(const msgb_mswpt *plan, const double *coeffs, int mode,
+                         int real_output, double *out, void *workspace,
+                         size_t workspace_bytes, msgb_stream_t stream);
+
+/* ---- top_n selection (forward_solver_utils.py:65-89) ------------------- */
+
+/* Selects the n largest keys; ties at the threshold keep the highest indices
+ * (jnp.argpartition semantics); emits them ordered by (key, index) ascending.
+ * idx: (n) int64; values: (n) complex gathered from coeffs. */
+size_t msgb_topn_workspace_size(int64_t total, int64_t n);
+int msgb_topn(const double *keys, const double *coeffs, int64_t total, int64_t n,
+              int64_t *idx, double *values, void *workspace, size_t workspace_bytes,
+              msgb_stream_t stream);
+
+/* ---- beam initialisation (forward_solver_utils.py:255-373) ------------- */
+
+typedef struct msgb_beam_out {
+    double *x0, *p0, *alpha, *a0, *omega;  /* layouts as in msgb_beam_set */
+    double *a0_unit;                        /* (n) complex, optional (NULL) */
+} msgb_beam_out;
+
+/* Beam data for n selected flat indices; values (complex, may be NULL) are
+ * multiplied into a0.  L: physical domain size per axis. */
+int msgb_beam_init(const msgb_mswpt *plan, const double *L, const int64_t *idx,
+                   const double *values, int64_t n, const msgb_beam_out *out,
+                   msgb_stream_t stream);
+
+/* ---- adjoint scatter to coefficient space ------------------------------ */
+
+/* G[idx[j]] += scale * g[j] for unique idx (no atomics needed); G must be
+ * zeroed by the caller.  Complex FP64. */
+int msgb_scatter_coeff_grad(const int64_t *idx, const double *g, int64_t n, double scale,
+                            const msgb_mswpt *plan, int apply_half_mask, double *G,
+                            msgb_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MSGB_H */

