@@ -291,7 +291,10 @@ class MSGBSolver:
             _lib.check(_lib.lib().msgb_adj_gather_f64(_lib.ref(pr), _lib.ref(bs), d.data_ptr(),
                                                       torch.view_as_real(g).data_ptr(), st), "msgb_adj_gather_f64")
             return g
-        d = as_device_f64(data, dev).to(torch.float32).reshape(pr.nt, pr.ns).contiguous()
+        if isinstance(data, torch.Tensor) and data.is_cuda and data.dtype == torch.float32:
+            d = data.reshape(pr.nt, pr.ns).contiguous()
+        else:
+            d = as_device_f64(data, dev).to(torch.float32).reshape(pr.nt, pr.ns).contiguous()
         cnt = torch.zeros(1, dtype=torch.int64, device=dev)
         opts = _lib.SumOpts(cutoff=self.cutoff, eval_count=cnt.data_ptr())
         nbytes = _lib.lib().msgb_sum_f32_workspace_size(_lib.ref(pr), bt.n)

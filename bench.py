@@ -1,0 +1,403 @@
+#!/usr/bin/env python
+"""Benchmark: MSGB forward + exact adjoint on one B200 (beamax config 2).
+
+Workload (the configuration the headline metric is quoted on that fits one
+GPU): 2D 512 x 512 grid, dx = 1e-4 m, homogeneous c = 1500 m/s, cfl 0.3
+(Nt = 2414); 4 levels, boxes (4, 8, 16, 32), redundancy 2,
+rectangular_mirror; p0 = 64 seeded Gaussian wave packets (centres in the inner
+80 %, directions uniform, |k| uniform in each level's annulus, amplitudes
+N(0, 1)) + 8 Gaussian blobs (sigma 20 cells), max|p0| = 1; four-sided line
+sensor (2044 points); thr = 65536 top_n (131072 beams); solve_hom_diag.
+Synthetic data of those shapes; nothing is downloaded.
+
+A step = one forward (p0 -> sensor data) plus one exact adjoint (data ->
+image) on the FP32 path (Kahan sums, FP64 anchor phases, Gaussian cutoff).
+The dense FP64 path (reference semantics) is run once for comparison and as
+the accuracy reference.  ``value`` = dense-equivalent beam-sample evaluations
+per second of forward + adjoint (2 * 2n * Nt * Ns per step / step time).
+
+``--impl reference`` times the CPU restatement of the reference algorithm
+(C/OpenMP FP64, dense, all host threads) on a bounded beam sample and
+reports the same metric.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+adj beam-sample evaluations/s (dense-equivalent), FP32 path at <=1e-3 rel-L2 vs FP64"
+UNIT = "evals/s"
+
+
+# ---------------------------------------------------------------- workload
+def level_annuli(N, nbl, nl):
+    """Outer half-width (in Fourier index units) of every level's region."""
+    N_ref = min(N)
+    bls = [N_ref // (nbl[-1] * 2 ** L) for L in range(nl - 1, -1, -1)]
+    return [nbl[l] * bls[l] / 2 for l in range(nl)]
+
+
+def make_p0(N, nbl, n_packets, n_blobs, blob_sigma, seed):
+    rng = np.random.default_rng(seed)
+    d = len(N)
+    grids = np.meshgrid(*[np.arange(n, dtype=np.float64) for n in N], indexing="ij")
+    x = np.stack(grids, -1)
+    radii = [0.0] + level_annuli(N, nbl, len(nbl))
+    p0 = np.zeros(N)
+    Nm = min(N)
+    for i in range(n_packets):
+        lvl = i % len(nbl)
+        kmag = rng.uniform(max(radii[lvl], 1.0), radii[lvl + 1])
+        if d == 2:
+            th = rng.uniform(0, 2 * np.pi)
+            u = np.array([np.cos(th), np.sin(th)])
+        else:
+            v = rng.standard_normal(d)
+            u = v / np.linalg.norm(v)
+        c = (0.1 + 0.8 * rng.uniform(size=d)) * np.asarray(N)
+        band = max(radii[lvl + 1] - radii[lvl], 1.0)
+        width = Nm / (np.pi * band)
+        r = x - c
+        env = np.exp(-np.sum(r * r, -1) / (2 * width ** 2))
+        p0 += rng.standard_normal() * env * np.cos(2 * np.pi * kmag / Nm * (r @ u))
+    for _ in range(n_blobs):
+        c = (0.1 + 0.8 * rng.uniform(size=d)) * np.asarray(N)
+        r = x - c
+        p0 += rng.standard_normal() * np.exp(-np.sum(r * r, -1) / (2 * blob_sigma ** 2))
+    return p0 / np.max(np.abs(p0))
+
+
+def config2(seed=0, thr=65536):
+    import beamax_b200 as bb
+
+    N = (512, 512)
+    dom = bb.Domain(N=N, dx=(1e-4, 1e-4), periodic=(False, False), cfl=0.3, c=1500.0)
+    dec = bb.DyadicDecomposition(4, N, (4, 8, 16, 32), (1, 1))
+    wpt = bb.MSWPT(dec, 2, "rectangular_mirror")
+    mask = np.zeros(N)
+    mask[0, :] = mask[-1, :] = mask[:, 0] = mask[:, -1] = 1
+    sensors = bb.Sensor(dom, binary_mask=mask)
+    ts = dom.generate_time_domain()
+    p0 = make_p0(N, (4, 8, 16, 32), 64, 8, 20.0, seed)
+    return dict(name=f"config2: 2D 512^2 homogeneous, 4 levels (4,8,16,32), four-sided sensor, thr={thr}",
+                domain=dom, wpt=wpt, sensors=sensors, ts=ts, p0=p0, thr=thr)
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """Samples nvidia-smi SM clocks and throttle reasons while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._proc = None
+
+    def start(self):
+        try:
+            self._proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception:
+            self._proc = None
+
+    def _read(self):
+        for line in self._proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self._proc is not None:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except Exception:
+                self._proc.kill()
+        time.sleep(0.05)
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].strip() == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------- ours
+def launches_per_step(levels: int) -> int:
+    """Kernels of libmsgb launched per step (cuFFT's own kernels excluded)."""
+    fwd = levels + 1 + 2 + 1 + (1 + 2 + 1 + 1) + 1  # boxes, key bits, radix sort, take, init, prep(4), sum
+    adj = 1 + 5 + 1 + 1 + 1 + levels + 1 + 1        # init, prep+permute, gather, scatter, zero, boxes, synth, real
+    return fwd + adj
+
+
+def run_ours(args, rank, world, device):
+    import torch
+
+    import beamax_b200 as bb
+    from beamax_b200.solvers.msgb_solver import Selection
+
+    torch.cuda.set_device(device)
+    W = config2(seed=1234 + rank, thr=args.thr)
+    dom, wpt, sens, ts, p0 = W["domain"], W["wpt"], W["sensors"], W["ts"], W["p0"]
+    hom = bb.gb.gb_solvers.solve_hom_diag
+    s32 = bb.MSGBSolver(W["thr"], "top_n", 128, "spatial", hom, "scan_real", precision="fp32", cutoff=args.cutoff)
+    s64 = bb.MSGBSolver(W["thr"], "top_n", 128, "spatial", hom, "scan_real", precision="fp64")
+    p0_d = torch.from_numpy(p0).to(device)
+    nt, ns = ts.size, sens.positions.shape[0]
+    n = W["thr"]
+    dense_step = 2 * (2 * n) * nt * ns  # forward + adjoint, both modes
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)
+    rng = np.random.default_rng(99 + rank)
+    data_probe = torch.from_numpy(rng.standard_normal((nt, ns))).to(device)
+
+    def step():
+        y = s32.forward(p0_d, dom, sens, ts, wpt)
+        img = s32.adjoint(y, dom, sens, ts, wpt)
+        return y, img
+
+    # warm-up (also builds device plans and workspaces)
+    for _ in range(max(args.warmup, 1)):
+        step()
+    torch.cuda.synchronize()
+
+    # kernel timing of the two dominant kernels on the launching stream
+    st = torch.cuda.current_stream()
+    sel = s32.select(p0_d, dom, wpt)
+    bt = s32.beams(sel, dom, wpt)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    flush.zero_()
+    ev[0].record(st)
+    y32 = s32.sum_forward(bt, dom, sens, ts)
+    ev[1].record(st)
+    fwd_evals = s32.eval_count()
+    flush.zero_()
+    ev[2].record(st)
+    g32 = s32.gather_adjoint(bt, dom, sens, ts, data_probe)
+    ev[3].record(st)
+    torch.cuda.synchronize()
+    adj_evals = s32.eval_count()
+    t_fwd_kernel = ev[0].elapsed_time(ev[1]) / 1e3
+    t_adj_kernel = ev[2].elapsed_time(ev[3]) / 1e3
+
+    # timed region
+    if world > 1:
+        torch.distributed.barrier()
+    sampler = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    times = []
+    torch.cuda.synchronize()
+    for _ in range(args.steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        step()
+        b.record(st)
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b) / 1e3)
+    if world > 1:
+        torch.distributed.barrier()
+    total = float(np.sum(times))
+    if world > 1:
+        t = torch.tensor([total], dtype=torch.float64, device=device)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total = float(t.item())
+    clocks = sampler.stop() if sampler else None
+
+    # e2e through the public API with host buffers (H2D of p0, D2H of data,
+    # H2D of data, D2H of the image inside the timed region)
+    p0_host = torch.from_numpy(p0).pin_memory()
+    e2e = []
+    for _ in range(max(1, min(args.steps, 3))):
+        flush.zero_()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        y_host = s32.forward(p0_host.numpy(), dom, sens, ts, wpt)
+        img_host = s32.adjoint(y_host, dom, sens, ts, wpt)
+        b.record(st)
+        torch.cuda.synchronize()
+        e2e.append(a.elapsed_time(b) / 1e3)
+    e2e_t = float(np.mean(e2e))
+
+    result = {"rank": rank, "t_step": total / args.steps, "t_fwd_kernel": t_fwd_kernel, "t_adj_kernel": t_adj_kernel,
+              "fwd_evals": fwd_evals, "adj_evals": adj_evals, "dense_step": dense_step, "clocks": clocks,
+              "e2e_t": e2e_t, "h2d": p0.nbytes + nt * ns * 4, "d2h": nt * ns * 4 + p0.nbytes,
+              "levels": wpt.dyadic_decomp.num_levels, "workload": W["name"]}
+
+    # FP64 plain path (dense, reference semantics): once, also the accuracy reference
+    if rank == 0 and not args.no_fp64:
+        flush.zero_()
+        torch.cuda.synchronize()
+        a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        a.record(st)
+        y64 = s64.forward(p0_d, dom, sens, ts, wpt)
+        b.record(st)
+        img64 = s64.adjoint(y64, dom, sens, ts, wpt)
+        c.record(st)
+        torch.cuda.synchronize()
+        y32f, img32 = step()
+        result["fp64"] = {"fwd_s": a.elapsed_time(b) / 1e3, "adj_s": b.elapsed_time(c) / 1e3}
+        rel = lambda r, x: float(torch.linalg.norm(r - x.double()) / torch.linalg.norm(r))
+        result["rel_l2_fwd"] = rel(y64, y32f)
+        img32b = s32.adjoint(y64.float(), dom, sens, ts, wpt)
+        result["rel_l2_adj"] = rel(img64, img32b)
+        # dot test of the FP32 transpose
+        q = torch.from_numpy(np.random.default_rng(5).standard_normal(dom.N)).to(device)
+        cq = wpt.forward_device(q, scale=0.5, half_mask=True)
+        selq = Selection(s32.last_selection.idx, cq[s32.last_selection.idx], wpt.total_coeffs)
+        Aq = s32.sum_forward(s32.beams(selq, dom, wpt), dom, sens, ts).double()
+        At = s32.adjoint(data_probe, dom, sens, ts, wpt, selection=s32.last_selection)
+        lhs, rhs = float((Aq * data_probe).sum()), float((q * At).sum())
+        result["dot_test_rel"] = abs(lhs - rhs) / abs(lhs)
+    return result
+
+
+def cpu_reference(args, workload_only=False):
+    """Dense FP64 C/OpenMP restatement on a bounded beam sample (all host threads)."""
+    import oracle.build as ob
+    from oracle import msgb as om
+
+    ob.build()
+    W = config2(seed=1234, thr=args.thr)
+    dom, wpt, sens, ts, p0 = W["domain"], W["wpt"], W["sensors"], W["ts"], W["p0"]
+    odom = om.Dom(N=dom.N, dx=dom.dx, periodic=dom.periodic, cfl=dom.cfl, c=1500.0)
+    dec = wpt.dyadic_decomp
+    ow = om.Wpt(om.Decomp(dec.num_levels, dec.N, dec.num_boxes_levels, dec.box_aspect_ratio), 2, wpt.windowing)
+    t0 = time.perf_counter()
+    bm = om.select_beams(p0, odom, ow, W["thr"])
+    t_select = time.perf_counter() - t0
+    nsample = args.cpu_sample
+    rng = np.random.default_rng(0)
+    pick = np.sort(rng.choice(bm.idx.size, size=nsample, replace=False))
+    sub = om.Beams(bm.idx[pick], bm.coeff[pick], bm.p0[pick], bm.M0[pick], bm.x0[pick], bm.omega[pick],
+                   bm.a0_unit[pick])
+    tab = om.beam_table(sub, 1500.0)
+    pos = sens.positions
+    t0 = time.perf_counter()
+    y = ob.sum_hom(tab, 1500.0, ts, pos, dom.grid_size, dom.periodic)
+    t_fwd = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ob.adj_hom(tab, sub.a0_unit, 1500.0, ts, pos, dom.grid_size, dom.periodic, y)
+    t_adj = time.perf_counter() - t0
+    evals = 2 * (2 * nsample) * ts.size * pos.shape[0]
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    value = evals / (t_fwd + t_adj)
+    full_s = (t_fwd + t_adj) * W["thr"] / nsample
+    return {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{nsample} of {W['thr']} selected coefficients ({2 * nsample} beams), all {ts.size} times x "
+                      f"{pos.shape[0]} sensors, dense FP64 forward + exact adjoint (C/OpenMP restatement); "
+                      f"full step extrapolated linearly in beams: {full_s:.1f} s",
+            "select_s": t_select, "t_fwd_s": t_fwd, "t_adj_s": t_adj, "workload": W["name"]}
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cutoff", type=float, default=16.0)
+    ap.add_argument("--thr", type=int, default=65536, help="top_n (65536 = config 2; smaller for profiling)")
+    ap.add_argument("--cpu-sample", type=int, default=96)
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        r = cpu_reference(args)
+        line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": r["workload"], "sample": r["sample"]},
+                "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import torch
+
+    if world > 1:
+        import datetime
+
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    device = torch.device("cuda", local_rank)
+    r = run_ours(args, rank, world, device)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return 0
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        try:
+            cpu = cpu_reference(args)
+            cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        except Exception as e:  # reported, never fatal
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {e}"}
+    t_step = r["t_step"]
+    value = world * r["dense_step"] / t_step
+    clk = r["clocks"] or {}
+    sm_mhz = clk.get("sm_mhz") or 1965.0
+    # FP32 roofline of the dominant kernel (forward summation): 36 flops per evaluated
+    # (beam, time, sensor) triple (24 FP32 instructions, FMA = 2), peak = 148 SMs x 128 lanes
+    # x 2 flops x the median SM clock sampled under load.
+    flops_per_eval = 36.0
+    peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    achieved = r["fwd_evals"] * flops_per_eval / r["t_fwd_kernel"] / 1e12
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": r["workload"], "global_batch": world, "parallelism": f"replicas{world}",
+                   "l2": "flushed (256 MiB write) between timed steps", "cutoff_efolds": args.cutoff},
+        "e2e": {"value": world * r["dense_step"] / r["e2e_t"], "unit": UNIT, "h2d_bytes_per_step": r["h2d"],
+                "d2h_bytes_per_step": r["d2h"], "ms_per_step": r["e2e_t"] * 1e3},
+        "gpu_launches": args.steps * launches_per_step(r["levels"]),
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "kernel": "fwd32_kernel", "flops_per_eval": flops_per_eval,
+                     "peak_basis": f"148 SM x 128 FP32 lanes x 2 x {sm_mhz:.0f} MHz (median sampled SM clock)"},
+        "kernels": {"fwd32_s": r["t_fwd_kernel"], "adj32_s": r["t_adj_kernel"], "fwd_evals": r["fwd_evals"],
+                    "adj_evals": r["adj_evals"], "dense_evals_per_step": r["dense_step"],
+                    "fwd_evals_per_s": r["fwd_evals"] / r["t_fwd_kernel"],
+                    "adj_evals_per_s": r["adj_evals"] / r["t_adj_kernel"]},
+        "clocks": clk,
+        "cpu_baseline": cpu,
+    }
+    if "fp64" in r:
+        f = r["fp64"]
+        line["fp64_plain"] = {"fwd_ms": f["fwd_s"] * 1e3, "adj_ms": f["adj_s"] * 1e3,
+                              "value": r["dense_step"] / (f["fwd_s"] + f["adj_s"]),
+                              "speedup_fp32_vs_fp64": (f["fwd_s"] + f["adj_s"]) / t_step}
+        line["rel_l2_fwd_vs_fp64"] = r["rel_l2_fwd"]
+        line["rel_l2_adj_vs_fp64"] = r["rel_l2_adj"]
+        line["dot_test_rel_fp32"] = r["dot_test_rel"]
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -302,8 +302,24 @@ class Wpt:
         self.windowing = windowing
         mesh = dec.fourier_meshgrid
         ssq = np.zeros(dec.N)
-        for i in range(dec.total_num_boxes):
-            ssq = ssq + np.square(filter_idx(dec, i, redundancy, windowing))
+        Nv0 = np.asarray(dec.N)
+        sup = [dec.box_lengths[l] * np.asarray(dec.box_aspect_ratio) * redundancy for l in range(dec.num_levels)]
+        if windowing != "none" and all(np.all(s <= Nv0) for s in sup):
+            # Windowed filters vanish outside their box's support patch, so the
+            # full-grid sum (transforms.py:511-555) only receives +0.0 elsewhere;
+            # accumulating over the patches alone gives the same values.
+            for i in range(dec.total_num_boxes):
+                lvl = int(dec.find_level(i))
+                S = sup[lvl]
+                c = dec.centres_ndim[i]
+                j = np.stack(np.meshgrid(*[np.arange(x) for x in S], indexing="ij"), -1)
+                kg = (c + Nv0 // 2 - S // 2 + j) % Nv0
+                g = windowed_gaussian(c, kg - Nv0 // 2, dec.box_lengths[lvl], dec.box_aspect_ratio, dec.N,
+                                      redundancy, windowing)
+                ssq[tuple(np.moveaxis(kg, -1, 0))] += np.square(g)
+        else:
+            for i in range(dec.total_num_boxes):
+                ssq = ssq + np.square(filter_idx(dec, i, redundancy, windowing))
         if not np.all(np.isfinite(ssq)) or not np.all(ssq > 0):
             raise ValueError("The dyadic decomposition leaves uncovered Fourier bins.")
         self.sum_gsquare = ssq
