@@ -34,8 +34,12 @@ class BeamSet(ctypes.Structure):
                 ("omega", c_vp)]
 
 
+class SensorTiling(ctypes.Structure):
+    _fields_ = [("n_tiles", c_i64), ("order", c_vp), ("tile_offsets", c_vp)]
+
+
 class SumOpts(ctypes.Structure):
-    _fields_ = [("cutoff", c_dbl), ("eval_count", c_vp)]
+    _fields_ = [("cutoff", c_dbl), ("eval_count", c_vp), ("tiling", c_vp)]
 
 
 class MswptDesc(ctypes.Structure):

@@ -1,24 +1,31 @@
 // FP32 Gaussian-beam summation with Gaussian-cutoff culling, and its transpose.
 //
 // Same operator as compute_gaussian_beam_real (beamax gb/core.py:194-329)
-// with solve_hom_diag (gb/gb_solvers.py:356-422), evaluated as
-//   out(t, s) = sum_b 2|A_b(t)| cos(theta_b(t, s)) exp(-chi_b(t, s)),
+// with solve_hom_diag (gb/gb_solvers.py:356-422):
+//   out(t, s) = sum_b Re[z_b(t, s)],  z = 2|A| exp(i theta - chi),
 //   theta = w (p.D + D^T Re M D / 2) + arg A,  chi = w D^T Im M D / 2,
 //   D = s - x_b(t).
-// Precision plan:
-//  * sensors are grouped into spatially compact tiles (Morton order); each tile
-//    has an FP64 anchor s0.  Per (beam, time) the large phase w p.(s0 - x(t)) +
-//    arg A is formed in FP64 and reduced to [-pi, pi) before it meets FP32;
-//    per sensor only w p.(s - s0) (bounded by the tile size) is FP32.
-//  * evaluation is FP32 (MUFU exp2 / cos after explicit range reduction),
-//    accumulation across beams is Kahan-compensated FP32.
-// Culling: for a (beam, time tile, sensor tile) triple the exponent satisfies
+//
+// Precision plan
+//  * Sensors are grouped into tiles of TS sensors, ordered so that tiles hold
+//    straight, evenly spaced runs (coarse-cell Morton order, row-major inside a
+//    cell).  Each tile has an FP64 anchor s0.  Per (beam, time) the large phase
+//    w p.(s0 - x(t)) + arg A is formed in FP64 and reduced to [-pi, pi) before
+//    it meets FP32; per sensor only w p.(s - s0) (bounded by the tile) is FP32.
+//  * Along a run s_k = s_a + k h the exponent i theta - chi is a quadratic in k,
+//    so z_{k+1} = z_k r_k, r_{k+1} = r_k q with r_0 = exp(a1 + a2), q =
+//    exp(2 a2): two complex multiplies per sensor.  Every run starts with a
+//    direct evaluation (MUFU sincos/exp after explicit range reduction) and
+//    runs are at most GS sensors long, which bounds the recurrence's relative
+//    error growth (~k^2 eps / 2 < 1e-5).
+//  * Accumulation across beams is Kahan-compensated FP32.
+// Culling: for a (beam, time tile, sensor tile) triple
 //   chi >= (w/2) lambda_min(Im M(t)) |D|^2 >= (w/2) lam_lo(t_b) dist^2,
-// with lam_lo(t) = 1 / (1/beta_min + (c t/|p|)^2 beta_max) (M0 = i diag(beta):
-// Im M(t) = (S + R S^-1 R)^-1 with S = diag(1/beta), R = (c t/|p|) P_perp, so
-// Im M is Loewner-decreasing in |t|) and dist the gap between the bounding
-// boxes of the centre's path over the time tile and of the sensor tile.  A
-// triple is skipped when that bound exceeds `cutoff` e-folds.
+// lam_lo(t) = 1 / (1/beta_min + (c t/|p|)^2 beta_max): with M0 = i diag(beta),
+// Im M(t) = (S + R S^-1 R)^-1, S = diag(1/beta), R = (c t/|p|) P_perp, which is
+// Loewner-decreasing in |t|; dist is the gap between the bounding boxes of the
+// centre's path over the time tile and of the sensor tile.  A triple is
+// skipped when that bound exceeds `cutoff` e-folds.
 #include <cub/cub.cuh>
 
 #include "common.cuh"
@@ -26,22 +33,16 @@
 namespace msgb {
 namespace {
 
-constexpr int TS = 64;    // sensors per tile
-constexpr int TT = 32;    // times per tile
-constexpr int THREADS = 256;
-constexpr int G = THREADS / TT;  // beams per record group
-constexpr int SPT = TS / (THREADS / TT);  // sensors per thread (forward)
+constexpr int TT = 32;               // times per tile (= lanes)
+constexpr int GS = 16;               // sensors per warp group and maximal run length
+constexpr int NW = 8;                // warps per CTA (forward)
+constexpr int TS = GS * NW;          // sensors per tile
+constexpr int THREADS = NW * 32;
+constexpr int G = THREADS / TT;      // beams per record pass
 constexpr float kTwoPi = 6.283185307179586f;
 constexpr float kInvTwoPi = 0.15915494309189535f;
-constexpr float kLog2e = 1.4426950408889634f;
 
-__device__ __forceinline__ float ex2_approx(float x) {
-    float y;
-    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-
-// Reduce an FP32 angle to [-pi, pi] (bounded inputs, |theta| < 2^20).
+// Reduce an FP32 angle to [-pi, pi] (bounded inputs).
 __device__ __forceinline__ float reduce_angle(float th) {
     const float k = rintf(th * kInvTwoPi);
     return fmaf(-k, kTwoPi, th);
@@ -50,7 +51,9 @@ __device__ __forceinline__ float reduce_angle(float th) {
 struct cf {
     float re, im;
 };
-__device__ __forceinline__ cf cmul(cf a, cf b) { return cf{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+__device__ __forceinline__ cf cmul(cf a, cf b) {
+    return cf{fmaf(a.re, b.re, -a.im * b.im), fmaf(a.re, b.im, a.im * b.re)};
+}
 __device__ __forceinline__ cf cdiv(cf a, cf b) {
     const float inv = __frcp_rn(fmaf(b.re, b.re, b.im * b.im));
     return cf{(a.re * b.re + a.im * b.im) * inv, (a.im * b.re - a.re * b.im) * inv};
@@ -62,16 +65,62 @@ __device__ __forceinline__ cf csqrtf_(cf z) {
     if (z.re >= 0.0f) return cf{r, z.im / (2.0f * r)};
     return cf{fabsf(z.im) / (2.0f * r), copysignf(r, z.im)};
 }
+// exp(x + i y) with y range-reduced first.
+__device__ __forceinline__ cf cexpf_(float x, float y) {
+    float s, c;
+    __sincosf(reduce_angle(y), &s, &c);
+    const float e = __expf(x);
+    return cf{e * c, e * s};
+}
+
+template <int D>
+struct Sym {
+    static constexpr int S = D * (D + 1) / 2;
+};
+
+// Quadratic form with packed coefficients (off-diagonals already doubled).
+template <int D>
+__device__ __forceinline__ float quad(const float *c, const float *v) {
+    float r = 0.0f;
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int k = i; k < D; ++k) r = fmaf(c[sym_index<D>(i, k)], v[i] * v[k], r);
+    return r;
+}
+// 2 u^T C v for the same packed coefficients.
+template <int D>
+__device__ __forceinline__ float bilin2(const float *c, const float *u, const float *v) {
+    float r = 0.0f;
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int k = i; k < D; ++k) {
+            const float ck = c[sym_index<D>(i, k)];
+            r = (i == k) ? fmaf(2.0f * ck, u[i] * v[i], r) : fmaf(ck, fmaf(u[i], v[k], u[k] * v[i]), r);
+        }
+    return r;
+}
 
 // Per (beam, time) evaluation record.
 template <int D>
 struct Rec {
-    float d0[D];                // s0 - x(t)
-    float q[D * (D + 1) / 2];   // w/2 Re M (off-diagonals doubled)
-    float e[D * (D + 1) / 2];   // -log2(e) w/2 Im M (off-diagonals doubled)
-    float wp[D];                // w p
-    float th0;                  // reduce(w p.(s0 - x(t)) + arg A)
-    float amp;                  // 2 |A(t)|
+    float d0[D];             // s0 - x(t)
+    float wp[D];             // w p
+    float q[Sym<D>::S];      // w/2 Re M (off-diagonals doubled)
+    float p[Sym<D>::S];      // w/2 Im M (off-diagonals doubled)
+    float th0;               // reduce(w p.(s0 - x(t)) + arg A)
+    float amp;               // 2 |A(t)|
+    static constexpr int NF = 2 * D + 2 * Sym<D>::S + 2;
+};
+
+// Tile-independent part of a record (the FP64 centre and the FP32 shape).
+template <int D>
+struct BeamTime {
+    double x[D];
+    double wp[D];
+    float q[Sym<D>::S], p[Sym<D>::S];
+    float ang, amp;
 };
 
 // Per selected coefficient culling data (mode independent).
@@ -89,11 +138,9 @@ struct TileInfo {
     float lo[D], hi[D];
 };
 
-// Closed-form beam state in FP32 (gb_solvers.py:306-353, :194-264) for the
-// Hessian and the amplitude; the centre is formed in FP64 by the caller.
+// Closed-form Hessian and amplitude in FP32 (gb_solvers.py:306-353, :194-264).
 template <int D>
-__device__ __forceinline__ void hom_mA_f32(const float *p0, const cf *al, cf a0, float c0t,
-                                           cf *M, cf &A) {
+__device__ __forceinline__ void hom_mA_f32(const float *p0, const cf *al, cf a0, float c0t, cf *M, cf &A) {
     float n2 = 0.0f;
 #pragma unroll
     for (int i = 0; i < D; ++i) n2 = fmaf(p0[i], p0[i], n2);
@@ -146,9 +193,10 @@ __device__ __forceinline__ void hom_mA_f32(const float *p0, const cf *al, cf a0,
     }
 }
 
+// Beam b in [0, 2n) (b >= n: mode -1) at time t, anchor-independent part.
 template <int D>
-__device__ __forceinline__ void make_rec(const ProbArgs &P, const BeamArgs &B, int64_t b, double t,
-                                         const double *s0, Rec<D> &r) {
+__device__ __forceinline__ void beam_time(const ProbArgs &P, const BeamArgs &B, int64_t b, double t,
+                                          BeamTime<D> &r) {
     const int64_t j = b < B.n ? b : b - B.n;
     const double c0 = b < B.n ? P.c : -P.c;
     double p0d[D], n2 = 0.0;
@@ -159,22 +207,18 @@ __device__ __forceinline__ void make_rec(const ProbArgs &P, const BeamArgs &B, i
     }
     const double np = sqrt(n2);
     const double w = B.omega[j];
-    double lin = 0.0;
     float p0f[D];
     cf al[D];
 #pragma unroll
     for (int i = 0; i < D; ++i) {
         double x = B.x0[j * D + i] + c0 * (p0d[i] / np) * t;
         if (P.periodic[i]) x = pymod(x, P.L[i]);
-        double d0 = s0[i] - x;
-        if (P.periodic[i]) d0 -= P.L[i] * nearbyint(d0 / P.L[i]);
-        r.d0[i] = (float)d0;
-        lin = fma(w * p0d[i], d0, lin);
-        r.wp[i] = (float)(w * p0d[i]);
+        r.x[i] = x;
+        r.wp[i] = w * p0d[i];
         p0f[i] = (float)p0d[i];
         al[i] = cf{(float)B.alpha[2 * (j * D + i)], (float)B.alpha[2 * (j * D + i) + 1]};
     }
-    cf M[D * (D + 1) / 2], A;
+    cf M[Sym<D>::S], A;
     hom_mA_f32<D>(p0f, al, cf{(float)B.a0[2 * j], (float)B.a0[2 * j + 1]}, (float)(c0 * t), M, A);
     const float wf = (float)w;
 #pragma unroll
@@ -184,18 +228,69 @@ __device__ __forceinline__ void make_rec(const ProbArgs &P, const BeamArgs &B, i
             const int q = sym_index<D>(i, k);
             const float f = (i == k ? 0.5f : 1.0f) * wf;
             r.q[q] = f * M[q].re;
-            r.e[q] = -kLog2e * f * M[q].im;
+            r.p[q] = f * M[q].im;
         }
     float re = A.re;
     if (A.re == 0.0f && A.im == 0.0f) re = 1e-12f;
-    const double th = lin + (double)atan2f(A.im, re);
-    r.th0 = (float)(th - 6.283185307179586 * nearbyint(th * 0.15915494309189535));
+    r.ang = atan2f(A.im, re);
     r.amp = 2.0f * sqrtf(fmaf(A.re, A.re, A.im * A.im));
 }
 
+// Anchor-dependent completion of a record.
 template <int D>
-__device__ __forceinline__ bool survives(const Cull<D> &cb, float c0, float ta, float tb,
-                                         const TileInfo<D> &ti, const ProbArgs &P, float cutoff) {
+__device__ __forceinline__ void anchor(const ProbArgs &P, const BeamTime<D> &bt, const double *s0, Rec<D> &r) {
+    double lin = 0.0;
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+        double d0 = s0[i] - bt.x[i];
+        if (P.periodic[i]) d0 -= P.L[i] * nearbyint(d0 / P.L[i]);
+        r.d0[i] = (float)d0;
+        r.wp[i] = (float)bt.wp[i];
+        lin = fma(bt.wp[i], d0, lin);
+    }
+#pragma unroll
+    for (int q = 0; q < Sym<D>::S; ++q) {
+        r.q[q] = bt.q[q];
+        r.p[q] = bt.p[q];
+    }
+    const double th = lin + (double)bt.ang;
+    r.th0 = (float)(th - 6.283185307179586 * nearbyint(th * 0.15915494309189535));
+    r.amp = bt.amp;
+}
+
+// Direct evaluation at a run start (seed): z, and the recurrence factors for
+// the step h to the next sensor.
+template <int D, bool PERIODIC>
+__device__ __forceinline__ cf seed_eval(const Rec<D> &r, const float *ds, const float *h, bool cont,
+                                        const ProbArgs &P, cf &rr, cf &qq) {
+    float Dl[D];
+    float th = r.th0;
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+        Dl[i] = ds[i] + r.d0[i];
+        if (PERIODIC && P.periodic[i]) Dl[i] -= (float)P.L[i] * rintf(Dl[i] / (float)P.L[i]);
+        th = fmaf(r.wp[i], ds[i], th);
+    }
+    th += quad<D>(r.q, Dl);
+    const float chi = quad<D>(r.p, Dl);
+    cf z = cexpf_(-chi, th);
+    z.re *= r.amp;
+    z.im *= r.amp;
+    if (cont) {
+        float wh = 0.0f;
+#pragma unroll
+        for (int i = 0; i < D; ++i) wh = fmaf(r.wp[i], h[i], wh);
+        const float a1r = -bilin2<D>(r.p, h, Dl), a1i = wh + bilin2<D>(r.q, h, Dl);
+        const float a2r = -quad<D>(r.p, h), a2i = quad<D>(r.q, h);
+        rr = cexpf_(a1r + a2r, a1i + a2i);
+        qq = cexpf_(2.0f * a2r, 2.0f * a2i);
+    }
+    return z;
+}
+
+template <int D>
+__device__ __forceinline__ bool survives(const Cull<D> &cb, float c0, float ta, float tb, const TileInfo<D> &ti,
+                                         const ProbArgs &P, float cutoff) {
     if (!cb.ok || cutoff <= 0.0f) return true;
     float d2 = 0.0f;
 #pragma unroll
@@ -213,11 +308,15 @@ __device__ __forceinline__ bool survives(const Cull<D> &cb, float c0, float ta, 
 }
 
 // ------------------------------------------------------------------ prep
+// Sort key: Morton order of coarse cells (32 per axis), row-major inside a
+// cell, so axis-aligned lines and planes form evenly spaced runs.
 template <int D>
-__global__ void morton_kernel(const double *sens, int64_t ns, ProbArgs P, uint32_t *key, int32_t *val) {
+__global__ void sensor_key_kernel(const double *sens, int64_t ns, ProbArgs P, uint32_t *key, int32_t *val) {
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (s >= ns) return;
     const int bits = D == 1 ? 31 : (D == 2 ? 16 : 10);
+    const int cellbits = 5;
+    const int lowbits = bits - cellbits;
     uint32_t q[D];
 #pragma unroll
     for (int i = 0; i < D; ++i) {
@@ -226,27 +325,41 @@ __global__ void morton_kernel(const double *sens, int64_t ns, ProbArgs P, uint32
         q[i] = (uint32_t)(u * (double)(1u << bits));
     }
     uint32_t k = 0;
-    for (int b = bits - 1; b >= 0; --b)
+    if (D == 1) {
+        k = q[0];
+    } else {
+        for (int b = cellbits - 1; b >= 0; --b)
 #pragma unroll
-        for (int i = 0; i < D; ++i) k = (k << 1) | ((q[i] >> b) & 1u);
+            for (int i = 0; i < D; ++i) k = (k << 1) | ((q[i] >> (lowbits + b)) & 1u);
+#pragma unroll
+        for (int i = 0; i < D; ++i) k = (k << lowbits) | (q[i] & ((1u << lowbits) - 1u));
+    }
     key[s] = k;
     val[s] = (int32_t)s;
 }
 
+// Per tile: anchor, bounding box, FP32 offsets, steps, run starts and the
+// per-group fast flag (one straight run of GS sensors, no periodic wrap).
 template <int D>
-__global__ void tile_kernel(const double *sens, int64_t ns, const int32_t *perm, TileInfo<D> *tiles,
-                            float *ds, double *sorted) {
+__global__ void tile_kernel(const double *sens, const int32_t *perm, const int32_t *offs, ProbArgs P,
+                            TileInfo<D> *tiles, float *ds, float *hn, uint8_t *seed, uint8_t *gfast,
+                            double *sorted) {
     const int64_t tile = blockIdx.x;
-    const int64_t first = tile * TS;
-    const int64_t cnt = min((int64_t)TS, ns - first);
+    const int64_t first = offs[tile];
+    const int cnt = offs[tile + 1] - offs[tile];
     __shared__ double lo[D], hi[D];
+    __shared__ double pos[TS][D];
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x)
+        for (int i = 0; i < D; ++i) pos[k][i] = sens[(int64_t)perm[first + k] * D + i];
+    __syncthreads();
+    bool any_periodic = false;
+    for (int i = 0; i < D; ++i) any_periodic |= (P.periodic[i] != 0);
     if (threadIdx.x == 0) {
         for (int i = 0; i < D; ++i) {
             double a = 1e300, b = -1e300;
-            for (int64_t k = 0; k < cnt; ++k) {
-                const double v = sens[(int64_t)perm[first + k] * D + i];
-                a = fmin(a, v);
-                b = fmax(b, v);
+            for (int k = 0; k < cnt; ++k) {
+                a = fmin(a, pos[k][i]);
+                b = fmax(b, pos[k][i]);
             }
             lo[i] = a;
             hi[i] = b;
@@ -254,15 +367,51 @@ __global__ void tile_kernel(const double *sens, int64_t ns, const int32_t *perm,
             tiles[tile].lo[i] = (float)a;
             tiles[tile].hi[i] = (float)b;
         }
-    }
-    __syncthreads();
-    for (int64_t k = threadIdx.x; k < cnt; k += blockDim.x) {
-        for (int i = 0; i < D; ++i) {
-            const double v = sens[(int64_t)perm[first + k] * D + i];
-            ds[(first + k) * D + i] = (float)(v - 0.5 * (lo[i] + hi[i]));
-            sorted[(first + k) * D + i] = v;
+        // run starts: a run continues while the step stays the same
+        bool have_h = false;
+        double hh[D];
+        unsigned fastmask = 0;
+        for (int k = 0; k < TS; ++k) {
+            bool s = true;
+            if (k < cnt) {
+                s = (k % GS == 0) || any_periodic;
+                if (!s) {
+                    double st[D], n2 = 0.0, e2 = 0.0;
+                    for (int i = 0; i < D; ++i) {
+                        st[i] = pos[k][i] - pos[k - 1][i];
+                        n2 += st[i] * st[i];
+                    }
+                    if (!have_h) {
+                        for (int i = 0; i < D; ++i) hh[i] = st[i];
+                        have_h = n2 > 0.0;
+                        s = !have_h;
+                    } else {
+                        for (int i = 0; i < D; ++i) e2 += (st[i] - hh[i]) * (st[i] - hh[i]);
+                        s = e2 > 1e-12 * n2;
+                    }
+                }
+                seed[first + k] = s ? 1 : 0;
+            }
+            if (s) have_h = false;
+            if (k % GS == 0) fastmask = 1;
+            if (k % GS != 0 && s) fastmask = 0;
+            if (k % GS == GS - 1) gfast[tile * NW + k / GS] = (fastmask && (k < cnt) && !any_periodic) ? 1 : 0;
         }
     }
+    __syncthreads();
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+        for (int i = 0; i < D; ++i) {
+            const double c = 0.5 * (lo[i] + hi[i]);
+            ds[(first + k) * D + i] = (float)(pos[k][i] - c);
+            hn[(first + k) * D + i] = (k + 1 < cnt) ? (float)(pos[k + 1][i] - pos[k][i]) : 0.0f;
+            sorted[(first + k) * D + i] = pos[k][i];
+        }
+    }
+}
+
+__global__ void fixed_offsets_kernel(int32_t *offs, int64_t n_tiles, int64_t ns) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i <= n_tiles) offs[i] = (int32_t)min((int64_t)i * TS, ns);
 }
 
 template <int D>
@@ -291,150 +440,195 @@ __global__ void cull_prep_kernel(BeamArgs B, Cull<D> *out) {
     out[j] = c;
 }
 
-__global__ void permute_rows_kernel(const float *data, const int32_t *perm, int64_t nt, int64_t ns, float *out) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= nt * ns) return;
-    const int64_t t = i / ns, s = i - t * ns;
-    out[i] = data[t * ns + perm[s]];
+// data (nt, ns) in caller order -> (ns, nt) in sorted sensor order.
+__global__ void transpose_permute_kernel(const float *data, const int32_t *perm, int64_t nt, int64_t ns, float *out) {
+    __shared__ float tile[32][33];
+    const int64_t s0 = (int64_t)blockIdx.x * 32, t0 = (int64_t)blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int64_t t = t0 + k, s = s0 + threadIdx.x;
+        tile[k][threadIdx.x] = (t < nt && s < ns) ? data[t * ns + perm[s]] : 0.0f;
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int64_t s = s0 + k, t = t0 + threadIdx.x;
+        if (s < ns && t < nt) out[s * nt + t] = tile[threadIdx.x][k];
+    }
 }
 
 // ------------------------------------------------------------------ forward
 template <int D>
-__global__ void __launch_bounds__(THREADS) fwd32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull,
-                                                        const TileInfo<D> *tiles, const float *ds,
-                                                        const int32_t *perm, float cutoff, float *out,
-                                                        unsigned long long *eval_count) {
-    __shared__ Rec<D> recs[G * TT];
-    __shared__ int64_t surv[THREADS * 2];
-    __shared__ int nsurv_s;
-    __shared__ int warp_cnt[THREADS / 32];
+__device__ __forceinline__ void load_rec(const float (*rec)[G][TT], int gl, int lane, Rec<D> &r) {
+    float *rf = reinterpret_cast<float *>(&r);
+#pragma unroll
+    for (int f = 0; f < Rec<D>::NF; ++f) rf[f] = rec[f][gl][lane];
+}
+
+__device__ __forceinline__ void kahan_add(float &acc, float &cmp, float v) {
+    const float y = v - cmp;
+    const float t = acc + y;
+    cmp = (t - acc) - y;
+    acc = t;
+}
+
+// Persistent CTAs take (time tile, sensor tile) work items from a counter.
+// Warp w owns sensor group w (GS sensors) of the tile; lane l owns time l.
+// Beams are evaluated two at a time (independent recurrence chains).
+template <int D, bool PERIODIC>
+__global__ void __launch_bounds__(THREADS, 2)
+fwd32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *tiles, const int32_t *offs,
+             const float *ds_g, const float *hn_g, const uint8_t *seed_g, const uint8_t *gfast_g,
+             const int32_t *perm, float cutoff, float *out, unsigned long long *eval_count, int *work, int n_st,
+             int n_tiles) {
+    constexpr int NF = Rec<D>::NF;
+    __shared__ float rec[NF][G][TT];
+    __shared__ float sds[TS][D], shn[TS][D];
+    __shared__ uint8_t sseed[TS + 1];
+    __shared__ int64_t surv[2 * THREADS];
+    __shared__ int warp_cnt[NW];
+    __shared__ int tile_s, nsurv_s;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int64_t st = blockIdx.x, tt = blockIdx.y;
-    const int64_t s_first = st * TS, t_first = tt * TT;
-    const int s_cnt = (int)min((int64_t)TS, P.ns - s_first);
-    const int t_cnt = (int)min((int64_t)TT, P.nt - t_first);
-    const TileInfo<D> ti = tiles[st];
-    const float ta = (float)P.ts[t_first], tb = (float)P.ts[t_first + t_cnt - 1];
-
-    const int tl = tid / (THREADS / TT);   // my time in the tile
-    const int sl = tid % (THREADS / TT);   // my sensor lane
-    float dsx[SPT][D];
-#pragma unroll
-    for (int k = 0; k < SPT; ++k) {
-        const int s = sl + k * (THREADS / TT);
-#pragma unroll
-        for (int i = 0; i < D; ++i) dsx[k][i] = s < s_cnt ? ds[(s_first + s) * D + i] : 0.0f;
-    }
-    float acc[SPT], cmp[SPT];
-#pragma unroll
-    for (int k = 0; k < SPT; ++k) acc[k] = 0.0f, cmp[k] = 0.0f;
     unsigned long long evals = 0;
+    while (true) {
+        if (tid == 0) tile_s = atomicAdd(work, 1);
+        __syncthreads();
+        const int tile = tile_s;
+        if (tile >= n_tiles) break;
+        const int64_t st = tile % n_st, tt = tile / n_st;
+        const int64_t s_first = offs[st], t_first = tt * TT;
+        const int s_cnt = offs[st + 1] - offs[st];
+        const int t_cnt = (int)min((int64_t)TT, P.nt - t_first);
+        const TileInfo<D> ti = tiles[st];
+        const float ta = (float)P.ts[t_first], tb = (float)P.ts[t_first + t_cnt - 1];
+        for (int k = tid; k < TS; k += THREADS) {
+#pragma unroll
+            for (int i = 0; i < D; ++i) {
+                sds[k][i] = k < s_cnt ? ds_g[(s_first + k) * D + i] : 0.0f;
+                shn[k][i] = k < s_cnt ? hn_g[(s_first + k) * D + i] : 0.0f;
+            }
+            sseed[k] = k < s_cnt ? seed_g[s_first + k] : 1;
+        }
+        if (tid == 0) sseed[TS] = 1;
+        const bool fast = gfast_g[st * NW + warp] != 0;
+        const int gbase = warp * GS;
+        const bool active = gbase < s_cnt;
+        float acc[GS], cmp[GS];
+#pragma unroll
+        for (int k = 0; k < GS; ++k) acc[k] = 0.0f, cmp[k] = 0.0f;
 
-    for (int64_t j0 = 0; j0 < B.n; j0 += THREADS) {
-        // 1. cull both modes of THREADS coefficients.
-        const int64_t j = j0 + tid;
-        bool keep_p = false, keep_m = false;
-        if (j < B.n) {
-            const Cull<D> cb = cull[j];
-            keep_p = survives<D>(cb, (float)P.c, ta, tb, ti, P, cutoff);
-            keep_m = survives<D>(cb, -(float)P.c, ta, tb, ti, P, cutoff);
-        }
-        const unsigned bp = __ballot_sync(0xffffffffu, keep_p);
-        const unsigned bm = __ballot_sync(0xffffffffu, keep_m);
-        if (lane == 0) warp_cnt[warp] = __popc(bp) + __popc(bm);
-        __syncthreads();
-        int off = 0, tot = 0;
-        for (int w = 0; w < THREADS / 32; ++w) {
-            if (w < warp) off += warp_cnt[w];
-            tot += warp_cnt[w];
-        }
-        const unsigned lt = (1u << lane) - 1u;
-        if (keep_p) surv[off + __popc(bp & lt)] = j;
-        if (keep_m) surv[off + __popc(bp) + __popc(bm & lt)] = j + B.n;
-        if (tid == 0) nsurv_s = tot;
-        __syncthreads();
-        const int nsurv = nsurv_s;
-        evals += (unsigned long long)nsurv;
-        // 2. evaluate survivors in groups of G beams x TT times.
-        for (int g0 = 0; g0 < nsurv; g0 += G) {
-            {
-                const int gl = tid / TT, tloc = tid % TT;
-                Rec<D> &r = recs[gl * TT + tloc];
-                if (g0 + gl < nsurv && tloc < t_cnt) {
-                    make_rec<D>(P, B, surv[g0 + gl], P.ts[t_first + tloc], ti.s0, r);
-                } else {
-                    r.amp = 0.0f;
-                    r.th0 = 0.0f;
-#pragma unroll
-                    for (int i = 0; i < D; ++i) r.d0[i] = 0.0f, r.wp[i] = 0.0f;
-#pragma unroll
-                    for (int q = 0; q < D * (D + 1) / 2; ++q) r.q[q] = 0.0f, r.e[q] = 0.0f;
-                }
+        for (int64_t j0 = 0; j0 < B.n; j0 += THREADS) {
+            const int64_t j = j0 + tid;
+            bool keep_p = false, keep_m = false;
+            if (j < B.n) {
+                const Cull<D> cb = cull[j];
+                keep_p = survives<D>(cb, (float)P.c, ta, tb, ti, P, cutoff);
+                keep_m = survives<D>(cb, -(float)P.c, ta, tb, ti, P, cutoff);
             }
+            const unsigned bp = __ballot_sync(0xffffffffu, keep_p);
+            const unsigned bm = __ballot_sync(0xffffffffu, keep_m);
+            if (lane == 0) warp_cnt[warp] = __popc(bp) + __popc(bm);
             __syncthreads();
-            const int ng = min(G, nsurv - g0);
-            for (int gl = 0; gl < ng; ++gl) {
-                const Rec<D> r = recs[gl * TT + tl];
+            int off = 0, tot = 0;
 #pragma unroll
-                for (int k = 0; k < SPT; ++k) {
-                    float Dl[D];
-                    float th = r.th0;
+            for (int w = 0; w < NW; ++w) {
+                if (w < warp) off += warp_cnt[w];
+                tot += warp_cnt[w];
+            }
+            const unsigned lt = (1u << lane) - 1u;
+            if (keep_p) surv[off + __popc(bp & lt)] = j;
+            if (keep_m) surv[off + __popc(bp) + __popc(bm & lt)] = j + B.n;
+            if (tid == 0) nsurv_s = tot;
+            __syncthreads();
+            const int nsurv = nsurv_s;
+            evals += (unsigned long long)nsurv * (unsigned long long)t_cnt * (unsigned long long)s_cnt;
+            for (int g0 = 0; g0 < nsurv; g0 += G) {
+                {
+                    const int gl = tid / TT, tloc = tid % TT;
+                    Rec<D> r;
+                    if (g0 + gl < nsurv && tloc < t_cnt) {
+                        BeamTime<D> bt;
+                        beam_time<D>(P, B, surv[g0 + gl], P.ts[t_first + tloc], bt);
+                        anchor<D>(P, bt, ti.s0, r);
+                    } else {
 #pragma unroll
-                    for (int i = 0; i < D; ++i) {
-                        Dl[i] = dsx[k][i] + r.d0[i];
-                        if (P.periodic[i]) Dl[i] -= (float)P.L[i] * rintf(Dl[i] / (float)P.L[i]);
-                        th = fmaf(r.wp[i], dsx[k][i], th);
+                        for (int i = 0; i < D; ++i) r.d0[i] = 0.0f, r.wp[i] = 0.0f;
+#pragma unroll
+                        for (int q = 0; q < Sym<D>::S; ++q) r.q[q] = 0.0f, r.p[q] = 0.0f;
+                        r.th0 = 0.0f;
+                        r.amp = 0.0f;
                     }
-                    float ex = 0.0f;
+                    const float *rf = reinterpret_cast<const float *>(&r);
 #pragma unroll
-                    for (int i = 0; i < D; ++i)
-#pragma unroll
-                        for (int m = i; m < D; ++m) {
-                            const int q = sym_index<D>(i, m);
-                            const float dd = Dl[i] * Dl[m];
-                            th = fmaf(r.q[q], dd, th);
-                            ex = fmaf(r.e[q], dd, ex);
-                        }
-                    const float v = r.amp * __cosf(reduce_angle(th)) * ex2_approx(ex);
-                    // Kahan-compensated accumulation across beams.
-                    const float y = v - cmp[k];
-                    const float tsum = acc[k] + y;
-                    cmp[k] = (tsum - acc[k]) - y;
-                    acc[k] = tsum;
+                    for (int f = 0; f < NF; ++f) rec[f][gl][tloc] = rf[f];
                 }
-            }
-            __syncthreads();
-        }
-    }
-    if (tl < t_cnt) {
-        const int64_t t = t_first + tl;
+                __syncthreads();
+                const int ng = min(G, nsurv - g0);
+                if (active) {
+                    for (int gl = 0; gl < ng; gl += 2) {
+                        Rec<D> ra, rb;
+                        load_rec<D>(rec, gl, lane, ra);
+                        load_rec<D>(rec, gl + 1, lane, rb);  // zero-amplitude record when gl + 1 == ng
+                        if (fast) {
+                            cf za, fa, qa, zb, fb, qb;
+                            za = seed_eval<D, false>(ra, sds[gbase], shn[gbase], true, P, fa, qa);
+                            zb = seed_eval<D, false>(rb, sds[gbase], shn[gbase], true, P, fb, qb);
+                            kahan_add(acc[0], cmp[0], za.re + zb.re);
 #pragma unroll
-        for (int k = 0; k < SPT; ++k) {
-            const int s = sl + k * (THREADS / TT);
-            if (s < s_cnt) out[t * P.ns + perm[s_first + s]] = acc[k] - cmp[k];
+                            for (int k = 1; k < GS; ++k) {
+                                za = cmul(za, fa);
+                                fa = cmul(fa, qa);
+                                zb = cmul(zb, fb);
+                                fb = cmul(fb, qb);
+                                kahan_add(acc[k], cmp[k], za.re + zb.re);
+                            }
+                        } else {
+                            cf dummy_r, dummy_q;
+#pragma unroll
+                            for (int k = 0; k < GS; ++k) {
+                                const int s = gbase + k;
+                                const cf za = seed_eval<D, PERIODIC>(ra, sds[s], shn[s], false, P, dummy_r, dummy_q);
+                                const cf zb = seed_eval<D, PERIODIC>(rb, sds[s], shn[s], false, P, dummy_r, dummy_q);
+                                kahan_add(acc[k], cmp[k], za.re + zb.re);
+                            }
+                        }
+                    }
+                }
+                __syncthreads();
+            }
         }
+        if (lane < t_cnt && active) {
+            const int64_t t = t_first + lane;
+#pragma unroll
+            for (int k = 0; k < GS; ++k) {
+                const int s = gbase + k;
+                if (s < s_cnt) out[t * P.ns + perm[s_first + s]] = acc[k] - cmp[k];
+            }
+        }
+        __syncthreads();
     }
-    if (eval_count && tid == 0 && evals)
-        atomicAdd(eval_count, evals * (unsigned long long)t_cnt * (unsigned long long)s_cnt);
+    if (eval_count && tid == 0 && evals) atomicAdd(eval_count, evals);
 }
 
 // ------------------------------------------------------------------ adjoint
-// One warp per selected coefficient (both modes).  Lanes test 32 sensor tiles
-// at a time, build 32 per-time records for a surviving tile in shared memory,
-// then evaluate two sensors each over the tile's times.
-template <int D>
-__global__ void __launch_bounds__(THREADS) adj32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull,
-                                                        const TileInfo<D> *tiles, const float *ds,
-                                                        const float *data_sorted, float cutoff,
-                                                        double *g, unsigned long long *eval_count) {
-    __shared__ Rec<D> recs_all[THREADS / 32][TT];
+// One warp per selected coefficient (both modes), lanes = the 32 times of a
+// time tile.  Lanes test 32 sensor tiles at a time; for each surviving tile
+// every lane accumulates d(t, s) conj(z) over the tile's sensors: groups that
+// are single runs are walked four at a time with interleaved recurrence
+// chains (data for the next sensor is loaded one step ahead), the others by
+// direct evaluation.  Data is in sorted-sensor-major layout (lanes read
+// consecutive times).  Per-tile FP32 partials go into FP64; the warp result is
+// reduced in a fixed order, so the output is deterministic.
+template <int D, bool PERIODIC>
+__global__ void __launch_bounds__(THREADS)
+adj32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *tiles, const int32_t *offs,
+             int64_t n_st, const float *ds_g, const float *hn_g, const uint8_t *gfast_g, const float *dataT,
+             float cutoff, double *g, unsigned long long *eval_count) {
+    constexpr int CH = 4;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t j = (int64_t)blockIdx.x * (THREADS / 32) + warp;
+    const int64_t j = (int64_t)blockIdx.x * NW + warp;
     if (j >= B.n) return;
-    Rec<D> *recs = recs_all[warp];
     const Cull<D> cb = cull[j];
-    const int64_t n_st = (P.ns + TS - 1) / TS, n_tt = (P.nt + TT - 1) / TT;
+    const int64_t n_tt = (P.nt + TT - 1) / TT;
     double gre = 0.0, gim = 0.0;
     unsigned long long evals = 0;
     for (int m = 0; m < 2; ++m) {
@@ -444,59 +638,82 @@ __global__ void __launch_bounds__(THREADS) adj32_kernel(ProbArgs P, BeamArgs B, 
             const int64_t t_first = tt * TT;
             const int t_cnt = (int)min((int64_t)TT, P.nt - t_first);
             const float ta = (float)P.ts[t_first], tb = (float)P.ts[t_first + t_cnt - 1];
+            const bool tv = lane < t_cnt;
+            const int64_t t = t_first + (tv ? lane : 0);
+            bool have_bt = false;
+            BeamTime<D> bt;
             for (int64_t st0 = 0; st0 < n_st; st0 += 32) {
                 const int64_t st_l = st0 + lane;
                 const bool keep = st_l < n_st && survives<D>(cb, c0, ta, tb, tiles[st_l], P, cutoff);
                 unsigned mask = __ballot_sync(0xffffffffu, keep);
+                if (mask && !have_bt) {
+                    beam_time<D>(P, B, b, P.ts[t], bt);
+                    have_bt = true;
+                }
                 while (mask) {
                     const int k = __ffs(mask) - 1;
                     mask &= mask - 1;
                     const int64_t st = st0 + k;
-                    const int64_t s_first = st * TS;
-                    const int s_cnt = (int)min((int64_t)TS, P.ns - s_first);
+                    const int64_t s_first = offs[st];
+                    const int s_cnt = offs[st + 1] - offs[st];
                     const TileInfo<D> ti = tiles[st];
-                    __syncwarp();
-                    if (lane < t_cnt) make_rec<D>(P, B, b, P.ts[t_first + lane], ti.s0, recs[lane]);
-                    __syncwarp();
+                    Rec<D> r;
+                    anchor<D>(P, bt, ti.s0, r);
+                    if (!tv) r.amp = 0.0f;
                     float pr = 0.0f, pi = 0.0f;
+                    const float *dcol = dataT + s_first * P.nt + t;
+                    const int ngroups = (s_cnt + GS - 1) / GS;
+                    unsigned fastbits = 0;
+                    for (int gq = 0; gq < ngroups; ++gq) fastbits |= (unsigned)(__ldg(gfast_g + st * NW + gq) != 0) << gq;
+                    int gq = 0;
+                    while (gq < ngroups) {
+                        if (gq + CH <= ngroups && ((fastbits >> gq) & ((1u << CH) - 1u)) == ((1u << CH) - 1u)) {
+                            cf z[CH], rr[CH], qq[CH];
+                            float d[CH];
 #pragma unroll
-                    for (int h = 0; h < TS / 32; ++h) {
-                        const int s = lane + 32 * h;
-                        if (s >= s_cnt) continue;
-                        float dsl[D];
+                            for (int c = 0; c < CH; ++c) {
+                                const int s = (gq + c) * GS;
+                                float dsl[D], hl[D];
 #pragma unroll
-                        for (int i = 0; i < D; ++i) dsl[i] = ds[(s_first + s) * D + i];
-                        const float *dcol = data_sorted + s_first + s;
-                        for (int tl = 0; tl < t_cnt; ++tl) {
-                            const Rec<D> &r = recs[tl];
-                            float Dl[D];
-                            float th = r.th0;
-#pragma unroll
-                            for (int i = 0; i < D; ++i) {
-                                Dl[i] = dsl[i] + r.d0[i];
-                                if (P.periodic[i]) Dl[i] -= (float)P.L[i] * rintf(Dl[i] / (float)P.L[i]);
-                                th = fmaf(r.wp[i], dsl[i], th);
+                                for (int i = 0; i < D; ++i)
+                                    dsl[i] = __ldg(ds_g + (s_first + s) * D + i), hl[i] = __ldg(hn_g + (s_first + s) * D + i);
+                                z[c] = seed_eval<D, false>(r, dsl, hl, true, P, rr[c], qq[c]);
+                                d[c] = tv ? __ldg(dcol + (int64_t)s * P.nt) : 0.0f;
                             }
-                            float ex = 0.0f;
+                            for (int kk = 0; kk < GS; ++kk) {
+                                float dn[CH];
 #pragma unroll
-                            for (int i = 0; i < D; ++i)
+                                for (int c = 0; c < CH; ++c)
+                                    dn[c] = (tv && kk + 1 < GS) ? __ldg(dcol + (int64_t)((gq + c) * GS + kk + 1) * P.nt) : 0.0f;
 #pragma unroll
-                                for (int q2 = i; q2 < D; ++q2) {
-                                    const int q = sym_index<D>(i, q2);
-                                    const float dd = Dl[i] * Dl[q2];
-                                    th = fmaf(r.q[q], dd, th);
-                                    ex = fmaf(r.e[q], dd, ex);
+                                for (int c = 0; c < CH; ++c) {
+                                    pr = fmaf(d[c], z[c].re, pr);
+                                    pi = fmaf(-d[c], z[c].im, pi);
+                                    z[c] = cmul(z[c], rr[c]);
+                                    rr[c] = cmul(rr[c], qq[c]);
+                                    d[c] = dn[c];
                                 }
-                            float sn, cs;
-                            __sincosf(reduce_angle(th), &sn, &cs);
-                            const float v = dcol[(t_first + tl) * P.ns] * r.amp * ex2_approx(ex);
-                            pr = fmaf(v, cs, pr);
-                            pi = fmaf(-v, sn, pi);
+                            }
+                            gq += CH;
+                        } else {
+                            const int s_end = min(s_cnt, (gq + 1) * GS);
+                            for (int s = gq * GS; s < s_end; ++s) {
+                                float dsl[D], hl[D];
+#pragma unroll
+                                for (int i = 0; i < D; ++i)
+                                    dsl[i] = __ldg(ds_g + (s_first + s) * D + i), hl[i] = 0.0f;
+                                cf dr, dq;
+                                const cf z = seed_eval<D, PERIODIC>(r, dsl, hl, false, P, dr, dq);
+                                const float d = tv ? __ldg(dcol + (int64_t)s * P.nt) : 0.0f;
+                                pr = fmaf(d, z.re, pr);
+                                pi = fmaf(-d, z.im, pi);
+                            }
+                            gq += 1;
                         }
                     }
                     gre += (double)pr;
                     gim += (double)pi;
-                    evals += (unsigned long long)t_cnt * (unsigned long long)s_cnt;
+                    evals += tv ? (unsigned long long)s_cnt : 0ull;
                 }
             }
         }
@@ -505,6 +722,7 @@ __global__ void __launch_bounds__(THREADS) adj32_kernel(ProbArgs P, BeamArgs B, 
     for (int o = 16; o > 0; o >>= 1) {
         gre += __shfl_down_sync(0xffffffffu, gre, o);
         gim += __shfl_down_sync(0xffffffffu, gim, o);
+        evals += __shfl_down_sync(0xffffffffu, evals, o);
     }
     if (lane == 0) {
         g[2 * j] = gre;
@@ -515,17 +733,23 @@ __global__ void __launch_bounds__(THREADS) adj32_kernel(ProbArgs P, BeamArgs B, 
 
 // ------------------------------------------------------------------ workspace
 struct Layout {
-    size_t keys_in, keys_out, vals_in, vals_out, cub, tiles, ds, sorted, cull, data, total;
+    size_t keys_in, keys_out, vals_in, vals_out, cub, tiles, offs, gfast, ds, hn, seed, sorted, cull, data, work, total;
     size_t cub_bytes;
+    int64_t n_st;
 };
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
-Layout layout(const msgb_problem *p, int64_t n_beams, bool with_data) {
+int64_t tile_count(const msgb_problem *p, const msgb_sum_opts *o) {
+    if (o && o->tiling) return o->tiling->n_tiles;
+    return (p->ns + TS - 1) / TS;
+}
+
+Layout layout(const msgb_problem *p, int64_t n_beams, bool with_data, int64_t n_st) {
     Layout l{};
     const int D = p->ndim;
     const int64_t ns = p->ns;
-    const int64_t n_st = (ns + TS - 1) / TS;
+    l.n_st = n_st;
     size_t cub_bytes = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, (const uint32_t *)nullptr, (uint32_t *)nullptr,
                                     (const int32_t *)nullptr, (int32_t *)nullptr, (int)ns);
@@ -537,61 +761,142 @@ Layout layout(const msgb_problem *p, int64_t n_beams, bool with_data) {
     l.vals_out = o; o = align256(o + ns * 4);
     l.cub = o; o = align256(o + cub_bytes);
     l.tiles = o; o = align256(o + n_st * sizeof(TileInfo<3>));
+    l.offs = o; o = align256(o + (n_st + 1) * 4);
+    l.gfast = o; o = align256(o + n_st * NW);
     l.ds = o; o = align256(o + ns * D * 4);
+    l.hn = o; o = align256(o + ns * D * 4);
+    l.seed = o; o = align256(o + ns + 1);
     l.sorted = o; o = align256(o + ns * D * 8);
     l.cull = o; o = align256(o + (n_beams > 0 ? n_beams : 1) * sizeof(Cull<3>));
     l.data = o; o = align256(o + (with_data ? p->nt * ns * 4 : 0));
+    l.work = o; o = align256(o + 64);
     l.total = o;
     return l;
 }
 
+__global__ void copy_i32_kernel(const int32_t *in, int64_t n, int32_t *out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) out[i] = in[i];
+}
+
+// Caller-provided tile offsets are clamped so that every tile lies in
+// [0, ns) and holds at most TS sensors; order entries outside [0, ns) are
+// replaced by 0.  (A malformed tiling gives wrong numbers, never an
+// out-of-bounds access.)
+__global__ void sanitize_tiling_kernel(const int32_t *offs_in, int64_t n_st, int64_t ns, int32_t *offs,
+                                       int32_t *order) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i <= n_st) {
+        int64_t v = offs_in[i];
+        v = v < 0 ? 0 : (v > ns ? ns : v);
+        offs[i] = (int32_t)v;
+    }
+    for (int64_t k = i; k < ns; k += (int64_t)gridDim.x * blockDim.x)
+        if (order[k] < 0 || order[k] >= ns) order[k] = 0;
+}
+
+__global__ void clamp_tiles_kernel(int32_t *offs, int64_t n_st) {
+    // serial pass (n_st is small): non-decreasing, at most TS per tile
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    for (int64_t i = 1; i <= n_st; ++i) {
+        int32_t lo = offs[i - 1];
+        int32_t v = offs[i] < lo ? lo : offs[i];
+        if (v - lo > TS) v = lo + TS;
+        offs[i] = v;
+    }
+}
+
 template <int D>
-int prep(const msgb_problem *p, const msgb_beam_set *b, const Layout &l, char *ws, cudaStream_t st) {
+int prep(const msgb_problem *p, const msgb_beam_set *b, const msgb_sum_opts *o, const Layout &l, char *ws,
+         cudaStream_t st) {
     const int64_t ns = p->ns;
     uint32_t *kin = (uint32_t *)(ws + l.keys_in), *kout = (uint32_t *)(ws + l.keys_out);
     int32_t *vin = (int32_t *)(ws + l.vals_in), *vout = (int32_t *)(ws + l.vals_out);
+    int32_t *offs = (int32_t *)(ws + l.offs);
     const int blk = 256;
-    morton_kernel<D><<<(unsigned)((ns + blk - 1) / blk), blk, 0, st>>>(p->sensors, ns, to_args(p), kin, vin);
-    size_t cb = l.cub_bytes;
-    cub::DeviceRadixSort::SortPairs(ws + l.cub, cb, kin, kout, vin, vout, (int)ns, 0, 32, st);
-    const int64_t n_st = (ns + TS - 1) / TS;
-    tile_kernel<D><<<(unsigned)n_st, 64, 0, st>>>(p->sensors, ns, vout, (TileInfo<D> *)(ws + l.tiles),
-                                                 (float *)(ws + l.ds), (double *)(ws + l.sorted));
+    if (o && o->tiling) {
+        if (!o->tiling->order || !o->tiling->tile_offsets || o->tiling->n_tiles <= 0)
+            return fail(MSGB_ERR_ARG, "sensor tiling: NULL arrays or no tiles");
+        copy_i32_kernel<<<(unsigned)((ns + blk - 1) / blk), blk, 0, st>>>(o->tiling->order, ns, vout);
+        sanitize_tiling_kernel<<<(unsigned)((l.n_st + 1 + blk - 1) / blk), blk, 0, st>>>(o->tiling->tile_offsets,
+                                                                                        l.n_st, ns, offs, vout);
+        clamp_tiles_kernel<<<1, 1, 0, st>>>(offs, l.n_st);
+    } else {
+        sensor_key_kernel<D><<<(unsigned)((ns + blk - 1) / blk), blk, 0, st>>>(p->sensors, ns, to_args(p), kin, vin);
+        size_t cb = l.cub_bytes;
+        cudaError_t e = cub::DeviceRadixSort::SortPairs(ws + l.cub, cb, kin, kout, vin, vout, (int)ns, 0, 32, st);
+        if (e != cudaSuccess) return fail(MSGB_ERR_CUDA, "sensor sort: %s", cudaGetErrorString(e));
+        fixed_offsets_kernel<<<(unsigned)((l.n_st + 1 + blk - 1) / blk), blk, 0, st>>>(offs, l.n_st, ns);
+    }
+    tile_kernel<D><<<(unsigned)l.n_st, 128, 0, st>>>(p->sensors, vout, offs, to_args(p), (TileInfo<D> *)(ws + l.tiles),
+                                                    (float *)(ws + l.ds), (float *)(ws + l.hn), (uint8_t *)(ws + l.seed),
+                                                    (uint8_t *)(ws + l.gfast), (double *)(ws + l.sorted));
     if (b->n > 0)
         cull_prep_kernel<D><<<(unsigned)((b->n + blk - 1) / blk), blk, 0, st>>>(to_args(b), (Cull<D> *)(ws + l.cull));
     return check_launch("msgb sum f32 prep");
 }
 
+int sm_count() {
+    int dev = 0, n = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n;
+}
+
 template <int D>
-int run_fwd(const msgb_problem *p, const msgb_beam_set *b, const msgb_sum_opts *o, char *ws,
-            const Layout &l, float *out, cudaStream_t st) {
-    if (int e = prep<D>(p, b, l, ws, st)) return e;
-    const int64_t n_st = (p->ns + TS - 1) / TS, n_tt = (p->nt + TT - 1) / TT;
-    if (n_tt > 65535) return fail(MSGB_ERR_UNSUPPORTED, "msgb_sum_fwd_f32: nt too large");
-    dim3 grid((unsigned)n_st, (unsigned)n_tt);
+int run_fwd(const msgb_problem *p, const msgb_beam_set *b, const msgb_sum_opts *o, char *ws, const Layout &l,
+            float *out, cudaStream_t st) {
+    if (int e = prep<D>(p, b, o, l, ws, st)) return e;
+    const int64_t n_st = l.n_st, n_tt = (p->nt + TT - 1) / TT;
+    if (n_st * n_tt > 0x7fffffffLL) return fail(MSGB_ERR_UNSUPPORTED, "msgb_sum_fwd_f32: too many tiles");
     ProbArgs P = to_args(p);
     P.sensors = (const double *)(ws + l.sorted);
-    fwd32_kernel<D><<<grid, THREADS, 0, st>>>(P, to_args(b), (const Cull<D> *)(ws + l.cull),
-                                               (const TileInfo<D> *)(ws + l.tiles), (const float *)(ws + l.ds),
-                                               (const int32_t *)(ws + l.vals_out), o ? (float)o->cutoff : 0.0f,
-                                               out, o ? o->eval_count : nullptr);
+    int *work = (int *)(ws + l.work);
+    cudaMemsetAsync(work, 0, sizeof(int), st);
+    bool periodic = false;
+    for (int i = 0; i < D; ++i) periodic |= (p->periodic[i] != 0);
+    const int n_tiles = (int)(n_st * n_tt);
+    const int64_t want = 2LL * sm_count();
+    const unsigned grid = (unsigned)(want < n_tiles ? want : n_tiles);
+    auto args = [&](auto kern) {
+        kern<<<grid, THREADS, 0, st>>>(P, to_args(b), (const Cull<D> *)(ws + l.cull), (const TileInfo<D> *)(ws + l.tiles),
+                                       (const int32_t *)(ws + l.offs), (const float *)(ws + l.ds),
+                                       (const float *)(ws + l.hn), (const uint8_t *)(ws + l.seed),
+                                       (const uint8_t *)(ws + l.gfast), (const int32_t *)(ws + l.vals_out),
+                                       o ? (float)o->cutoff : 0.0f, out, o ? o->eval_count : nullptr, work,
+                                       (int)n_st, n_tiles);
+    };
+    if (periodic)
+        args(fwd32_kernel<D, true>);
+    else
+        args(fwd32_kernel<D, false>);
     return check_launch("msgb_sum_fwd_f32");
 }
 
 template <int D>
-int run_adj(const msgb_problem *p, const msgb_beam_set *b, const msgb_sum_opts *o, char *ws,
-            const Layout &l, const float *data, double *g, cudaStream_t st) {
-    if (int e = prep<D>(p, b, l, ws, st)) return e;
-    const int64_t tot = p->nt * p->ns;
-    permute_rows_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(data, (const int32_t *)(ws + l.vals_out),
-                                                                     p->nt, p->ns, (float *)(ws + l.data));
+int run_adj(const msgb_problem *p, const msgb_beam_set *b, const msgb_sum_opts *o, char *ws, const Layout &l,
+            const float *data, double *g, cudaStream_t st) {
+    if (int e = prep<D>(p, b, o, l, ws, st)) return e;
+    dim3 tg((unsigned)((p->ns + 31) / 32), (unsigned)((p->nt + 31) / 32));
+    if (tg.y > 65535u) return fail(MSGB_ERR_UNSUPPORTED, "msgb_adj_gather_f32: nt too large");
+    transpose_permute_kernel<<<tg, dim3(32, 8), 0, st>>>(data, (const int32_t *)(ws + l.vals_out), p->nt, p->ns,
+                                                         (float *)(ws + l.data));
     ProbArgs P = to_args(p);
     P.sensors = (const double *)(ws + l.sorted);
-    const unsigned grid = (unsigned)((b->n + THREADS / 32 - 1) / (THREADS / 32));
-    adj32_kernel<D><<<grid, THREADS, 0, st>>>(P, to_args(b), (const Cull<D> *)(ws + l.cull),
-                                               (const TileInfo<D> *)(ws + l.tiles), (const float *)(ws + l.ds),
-                                               (const float *)(ws + l.data), o ? (float)o->cutoff : 0.0f, g,
-                                               o ? o->eval_count : nullptr);
+    bool periodic = false;
+    for (int i = 0; i < D; ++i) periodic |= (p->periodic[i] != 0);
+    const unsigned grid = (unsigned)((b->n + NW - 1) / NW);
+    auto args = [&](auto kern) {
+        kern<<<grid, THREADS, 0, st>>>(P, to_args(b), (const Cull<D> *)(ws + l.cull), (const TileInfo<D> *)(ws + l.tiles),
+                                       (const int32_t *)(ws + l.offs), l.n_st, (const float *)(ws + l.ds),
+                                       (const float *)(ws + l.hn), (const uint8_t *)(ws + l.gfast),
+                                       (const float *)(ws + l.data), o ? (float)o->cutoff : 0.0f, g,
+                                       o ? o->eval_count : nullptr);
+    };
+    if (periodic)
+        args(adj32_kernel<D, true>);
+    else
+        args(adj32_kernel<D, false>);
     return check_launch("msgb_adj_gather_f32");
 }
 
@@ -602,13 +907,17 @@ using namespace msgb;
 
 extern "C" size_t msgb_sum_f32_workspace_size(const msgb_problem *prob, int64_t n) {
     if (validate_problem(prob) || n < 0) return 0;
-    return layout(prob, n, true).total;
+    // The default tiling has the most tiles a valid tiling of ns sensors needs
+    // when every tile is full; reserve for one tile per 16 sensors so that
+    // caller tilings with partial tiles fit as well.
+    return layout(prob, n, true, (prob->ns + GS - 1) / GS).total;
 }
 
-static int check_ws(const msgb_problem *p, const msgb_beam_set *b, bool with_data, void *ws, size_t bytes,
-                    Layout &l) {
-    l = layout(p, b->n, with_data);
-    if (b->n > (int64_t(1) << 22)) return fail(MSGB_ERR_UNSUPPORTED, "at most 2^22 selected coefficients");
+static int check_ws(const msgb_problem *p, const msgb_beam_set *b, const msgb_sum_opts *o, bool with_data, void *ws,
+                    size_t bytes, Layout &l) {
+    l = layout(p, b->n, with_data, tile_count(p, o));
+    if (l.n_st <= 0) return fail(MSGB_ERR_ARG, "sensor tiling has no tiles");
+    if (b->n > (int64_t(1) << 26)) return fail(MSGB_ERR_UNSUPPORTED, "at most 2^26 selected coefficients");
     if (!ws || bytes < l.total)
         return fail(MSGB_ERR_WORKSPACE, "workspace too small: need %zu bytes, got %zu", l.total, bytes);
     if (((uintptr_t)ws & 255) != 0) return fail(MSGB_ERR_WORKSPACE, "workspace must be 256-byte aligned");
@@ -623,7 +932,7 @@ extern "C" int msgb_sum_fwd_f32(const msgb_problem *prob, const msgb_beam_set *b
     if (!out) return fail(MSGB_ERR_ARG, "msgb_sum_fwd_f32: out is NULL");
     if (prob->nt == 0 || prob->ns == 0) return MSGB_OK;
     Layout l;
-    if (int e = check_ws(prob, beams, false, workspace, workspace_bytes, l)) return e;
+    if (int e = check_ws(prob, beams, opts, false, workspace, workspace_bytes, l)) return e;
     cudaStream_t st = as_stream(stream);
     char *ws = (char *)workspace;
     switch (prob->ndim) {
@@ -645,7 +954,7 @@ extern "C" int msgb_adj_gather_f32(const msgb_problem *prob, const msgb_beam_set
         return check_launch("msgb_adj_gather_f32");
     }
     Layout l;
-    if (int e = check_ws(prob, beams, true, workspace, workspace_bytes, l)) return e;
+    if (int e = check_ws(prob, beams, opts, true, workspace, workspace_bytes, l)) return e;
     cudaStream_t st = as_stream(stream);
     char *ws = (char *)workspace;
     switch (prob->ndim) {

@@ -203,6 +203,26 @@ class MSGBSolver:
         pr.sensors = sd.data_ptr()
         return pr, (ts_d, sd)
 
+    def _tiling(self, domain: Domain, sensors, device):
+        """Run-based sensor tiling (cached per Sensor object), or None."""
+        import torch
+
+        from ..sensor_layout import build_tiling
+
+        def make():
+            t = build_tiling(self._sensor_positions(sensors), domain.dx)
+            if t is None:
+                return None
+            order, offs = t
+            od = torch.from_numpy(order).to(device)
+            fd = torch.from_numpy(offs).to(device)
+            st = _lib.SensorTiling(n_tiles=offs.size - 1, order=od.data_ptr(), tile_offsets=fd.data_ptr())
+            return st, od, fd
+
+        if isinstance(sensors, Sensor):
+            return _cache.get(sensors, ("tiling", str(device), tuple(domain.dx)), make)
+        return make()
+
     # ------------------------------------------------------------- pipeline
     def select(self, p0, domain: Domain, wpt: MSWPT, dpdt=None) -> Selection:
         """c_pos on the GPU, then top_n (msgb_solver.py:570-612)."""
@@ -269,7 +289,9 @@ class MSGBSolver:
             return out
         out = torch.empty((pr.nt, pr.ns), dtype=torch.float32, device=dev)
         cnt = torch.zeros(1, dtype=torch.int64, device=dev)
-        opts = _lib.SumOpts(cutoff=self.cutoff, eval_count=cnt.data_ptr())
+        tiling = self._tiling(domain, sensors, dev)
+        opts = _lib.SumOpts(cutoff=self.cutoff, eval_count=cnt.data_ptr(),
+                            tiling=_lib.ref(tiling[0]) if tiling else None)
         nbytes = _lib.lib().msgb_sum_f32_workspace_size(_lib.ref(pr), bt.n)
         ws = workspace(dev, "sum32", nbytes)
         _lib.check(_lib.lib().msgb_sum_fwd_f32(_lib.ref(pr), _lib.ref(bs), _lib.ref(opts), ws.data_ptr(), nbytes,
@@ -296,7 +318,9 @@ class MSGBSolver:
         else:
             d = as_device_f64(data, dev).to(torch.float32).reshape(pr.nt, pr.ns).contiguous()
         cnt = torch.zeros(1, dtype=torch.int64, device=dev)
-        opts = _lib.SumOpts(cutoff=self.cutoff, eval_count=cnt.data_ptr())
+        tiling = self._tiling(domain, sensors, dev)
+        opts = _lib.SumOpts(cutoff=self.cutoff, eval_count=cnt.data_ptr(),
+                            tiling=_lib.ref(tiling[0]) if tiling else None)
         nbytes = _lib.lib().msgb_sum_f32_workspace_size(_lib.ref(pr), bt.n)
         ws = workspace(dev, "sum32", nbytes)
         _lib.check(_lib.lib().msgb_adj_gather_f32(_lib.ref(pr), _lib.ref(bs), _lib.ref(opts), ws.data_ptr(), nbytes,
@@ -406,15 +430,26 @@ class MSGBSolver:
                 selection = self.last_selection
             else:
                 raise ValueError("adjoint needs a beam selection: call forward first or pass p0= or selection=")
-        bt = self.beams(selection, domain, wpt)
+        # Gather in flat-index order: neighbouring coefficients (same box,
+        # adjacent packet positions) have overlapping footprints, so the
+        # per-beam warps of a CTA reuse the same data tiles from L1.
+        order = torch_argsort(selection.idx)
+        sel_sorted = Selection(selection.idx[order], selection.values[order], selection.total_coeffs)
+        bt = self.beams(sel_sorted, domain, wpt)
         g = self.gather_adjoint(bt, domain, sensors, ts, data)
-        img = self.coefficient_adjoint(selection, g, wpt)
+        img = self.coefficient_adjoint(sel_sorted, g, wpt)
         return img if _is_torch(data) else img.cpu().numpy()
 
     def eval_count(self) -> Optional[int]:
         """Evaluated (beam, time, sensor) triples of the last FP32 call."""
         c = getattr(self, "_eval_counter", None)
         return None if c is None else int(c.item())
+
+
+def torch_argsort(x):
+    import torch
+
+    return torch.argsort(x)
 
 
 def _is_torch(x) -> bool:

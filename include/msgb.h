@@ -69,12 +69,24 @@ typedef struct msgb_beam_set {
     const double *omega;     /* (n) frequency |xi| */
 } msgb_beam_set;
 
+/* Optional sensor order for the FP32 summation (device pointers).  Tile i
+ * holds the sorted sensors order[tile_offsets[i] .. tile_offsets[i+1]) (at
+ * most 128); within a tile, groups of 16 consecutive sensors that lie on one
+ * straight, evenly spaced run are evaluated with a complex-exponential
+ * recurrence.  NULL: the library's own cell-Morton order. */
+typedef struct msgb_sensor_tiling {
+    int64_t n_tiles;
+    const int32_t *order;         /* (ns) sorted position -> caller's sensor index */
+    const int32_t *tile_offsets;  /* (n_tiles + 1) */
+} msgb_sensor_tiling;
+
 /* Options of the FP32 summation. */
 typedef struct msgb_sum_opts {
     double cutoff;           /* skip a (beam, tile) pair when the Gaussian exponent
                                 is provably above this many e-folds (<= 0: dense) */
     unsigned long long *eval_count; /* optional device counter: evaluated
                                 (beam, t, sensor) triples are added to it */
+    const msgb_sensor_tiling *tiling; /* optional (NULL) */
 } msgb_sum_opts;
 
 const char *msgb_last_error(void);
@@ -108,6 +120,81 @@ int msgb_sum_fwd_f32(const msgb_problem *prob, const msgb_beam_set *beams,
 int msgb_adj_gather_f32(const msgb_problem *prob, const msgb_beam_set *beams,
                         const msgb_sum_opts *opts, void *workspace, size_t workspace_bytes,
                         const float *data, double *g, msgb_stream_t stream);
+
+/* ---- heterogeneous media: RK4 beam propagation ------------------------- */
+
+#define MSGB_TIME_TILE 32          /* time samples per culling record */
+
+enum {
+    MSGB_MEDIUM_CONSTANT = 0,      /* c(x) = c */
+    MSGB_MEDIUM_LINEAR = 1,        /* n-linear interpolation of grid values */
+    MSGB_MEDIUM_BSPLINE3 = 2       /* cubic B-spline, coefficients prefiltered by the caller
+                                      (scipy.ndimage.spline_filter, as utils/interp.py:66-73) */
+};
+
+/* Sound speed for the RK4 path (utils/interp.py:158-263): grid point k_a sits
+ * at origin_a + k_a spacing_a; boundary 0 nearest (clamp), 1 wrap, 2 reflect,
+ * 3 mirror (utils/interp.py:78-98). */
+typedef struct msgb_medium {
+    int32_t kind;
+    int32_t boundary;
+    int32_t n[3];
+    double spacing[3];
+    double origin[3];
+    const double *coeffs;    /* device, prod(n) values (C order) */
+    double c;                /* kind CONSTANT */
+    double lam;              /* absorption lambda of coupled_rhs_absorption */
+} msgb_medium;
+
+/* Trajectory output for beams [b_first, b_first + nb) of the 2n beams (b >= n:
+ * mode -1).  Any pointer may be NULL.  The amplitude is integrated from 1.
+ *   rec64: (nt, nb) records of 2d + 2d^2 + 2 doubles: x, p, M (row-major,
+ *          re/im interleaved), A (re, im).
+ *   rec32: (nt, nb) records for the FP32 summation: x (d doubles, wrapped on
+ *          periodic axes), w p (d doubles), w/2 Re M and w/2 Im M packed
+ *          upper-triangular with doubled off-diagonals (d(d+1)/2 floats each),
+ *          arg A and 2|A| (floats).
+ *   cull:  (ceil(nt / MSGB_TIME_TILE), nb, 2d + 1) floats: bounding box of
+ *          the centre over each time tile (lo, hi) and (w/2) min lambda_min(Im M).
+ *   status: (nb) 0 ok, 1 non-finite state encountered. */
+typedef struct msgb_trajectories {
+    int64_t nb;
+    int64_t b_first;
+    double *rec64;
+    void *rec32;
+    float *cull;
+    int32_t *status;
+} msgb_trajectories;
+
+/* Fixed-step FP64 RK4 of coupled_rhs_absorption (gb/gb_solvers.py:787-867)
+ * with step (ts[1] - ts[0]) / substeps, state recorded at every ts. */
+int msgb_rk4_trajectories(const msgb_problem *prob, const msgb_medium *med, const msgb_beam_set *beams,
+                          int substeps, const msgb_trajectories *out, msgb_stream_t stream);
+
+/* Summation from trajectories (beams [b_first, b_first + nb) of traj).  The
+ * amplitude of beam b is a0[b mod n] times the trajectory's A.
+ * FP64: dense, accumulates (+=) into out (nt, ns) FP64, which the caller
+ * zeroes before the first chunk.
+ * FP32: culled by the trajectory's boxes; Kahan state (2 nt ns floats) lives in
+ * the workspace from the call with first_chunk != 0 to the call with
+ * last_chunk != 0, which writes out (nt, ns) FP32.  All chunks of one
+ * summation must use the same workspace and problem. */
+int msgb_sum_fwd_f64_traj(const msgb_problem *prob, const msgb_beam_set *beams,
+                          const msgb_trajectories *traj, double *out, msgb_stream_t stream);
+int msgb_adj_gather_f64_traj(const msgb_problem *prob, const msgb_beam_set *beams,
+                             const msgb_trajectories *traj, const double *data, double *g,
+                             msgb_stream_t stream);
+size_t msgb_sum_f32_traj_workspace_size(const msgb_problem *prob, int64_t nb_max);
+int msgb_sum_fwd_f32_traj(const msgb_problem *prob, const msgb_beam_set *beams,
+                          const msgb_trajectories *traj, const msgb_sum_opts *opts, int first_chunk,
+                          int last_chunk, void *workspace, size_t workspace_bytes, float *out,
+                          msgb_stream_t stream);
+/* g[b - b_first] for the chunk's beams (complex FP64, one entry per beam, not
+ * per coefficient: the caller adds the two modes). */
+int msgb_adj_gather_f32_traj(const msgb_problem *prob, const msgb_beam_set *beams,
+                             const msgb_trajectories *traj, const msgb_sum_opts *opts,
+                             void *workspace, size_t workspace_bytes, const float *data, double *g,
+                             msgb_stream_t stream);
 
 /* ---- MSWPT tiling (transforms.py:357-850) ------------------------------ */
 

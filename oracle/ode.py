@@ -1,0 +1,180 @@
+"""FP64 restatement of the heterogeneous beam ODE (test oracle).
+
+Test infrastructure: only ``tests/``, ``__graft_entry__.smoke`` and
+``bench.py``'s CPU legs use this module, as the checker.
+
+* ``GridSpeed`` restates ``make_c_function_from_grid`` (utils/interp.py:
+  31-263): linear or cubic B-spline tensor-product interpolation with SciPy's
+  ``spline_filter`` prefilter and the reference's boundary maps.  Gradient and
+  Hessian are the exact derivatives of that formula (what ``jax.grad`` /
+  ``jax.hessian`` of the same code return).
+* ``rhs`` restates ``coupled_rhs_absorption`` (gb/gb_solvers.py:787-867).
+* ``solve`` integrates it with SciPy DOP853 at a tight tolerance, the reference
+  test's own oracle (tests/test_gb.py:759-849), in place of diffrax Tsit5
+  (diffrax 0.7.2, gb_solvers.py:706-784), which is not installed here.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+from scipy import ndimage
+from scipy.integrate import solve_ivp
+
+_BOUNDARY = {"clamp": "nearest", "nearest": "nearest", "edge": "nearest", "reflect": "reflect",
+             "mirror": "mirror", "wrap": "wrap", "periodic": "wrap"}
+
+
+def map_indices(idx, n, boundary):
+    """utils/interp.py:78-98."""
+    if n == 1:
+        return np.zeros_like(idx)
+    if boundary == "nearest":
+        return np.clip(idx, 0, n - 1)
+    if boundary == "wrap":
+        return np.mod(idx, n)
+    if boundary == "reflect":
+        r = np.mod(idx, 2 * n)
+        return np.where(r < n, r, 2 * n - 1 - r)
+    if boundary == "mirror":
+        period = 2 * n - 2
+        r = np.mod(idx, period)
+        return np.where(r < n, r, period - r)
+    raise ValueError(boundary)
+
+
+def _weights(method, t):
+    """Weights and their first/second derivatives (utils/interp.py:101-118)."""
+    if method == "linear":
+        w = np.stack([1.0 - t, t], -1)
+        d1 = np.stack([-np.ones_like(t), np.ones_like(t)], -1)
+        d2 = np.zeros_like(w)
+        return w, d1, d2, (0, 1)
+    omt = 1.0 - t
+    t2, t3 = t * t, t * t * t
+    w = np.stack([omt ** 3 / 6.0, (3 * t3 - 6 * t2 + 4) / 6.0, (-3 * t3 + 3 * t2 + 3 * t + 1) / 6.0, t3 / 6.0], -1)
+    d1 = np.stack([-(omt ** 2) / 2.0, 1.5 * t2 - 2 * t, -1.5 * t2 + t + 0.5, t2 / 2.0], -1)
+    d2 = np.stack([omt, 3 * t - 2, -3 * t + 1, t], -1)
+    return w, d1, d2, (-1, 0, 1, 2)
+
+
+class GridSpeed:
+    """Sound speed interpolated from a grid, with gradient and Hessian."""
+
+    def __init__(self, c_map, spacing, origin=None, method="linear", boundary="clamp"):
+        self.values = np.asarray(c_map, dtype=np.float64)
+        d = self.values.ndim
+        self.spacing = np.asarray(spacing, float)
+        self.origin = np.zeros(d) if origin is None else np.asarray(origin, float)
+        self.method = method
+        self.boundary = _BOUNDARY[boundary]
+        if method == "bspline3":
+            self.coeffs = ndimage.spline_filter(self.values, order=3, mode=self.boundary)
+        elif method == "linear":
+            self.coeffs = self.values
+        else:
+            raise ValueError("method must be 'linear' or 'bspline3'.")
+
+    def eval(self, x):
+        """(c, grad c, hessian c) at one point x (d,)."""
+        d = self.coeffs.ndim
+        u = (np.asarray(x, float) - self.origin) / self.spacing
+        i0 = np.floor(u)
+        t = u - i0
+        w, d1, d2, offs = _weights(self.method, t)
+        n = len(offs)
+        c = 0.0
+        g = np.zeros(d)
+        H = np.zeros((d, d))
+        for corner in range(n ** d):
+            rem = corner
+            idx = []
+            loc = []
+            for ax in range(d):
+                k = rem % n
+                rem //= n
+                loc.append(k)
+                idx.append(int(map_indices(np.array(int(i0[ax]) + offs[k]), self.coeffs.shape[ax], self.boundary)))
+            v = self.coeffs[tuple(idx)]
+            wv = np.prod([w[ax, loc[ax]] for ax in range(d)])
+            c += wv * v
+            for a in range(d):
+                ga = d1[a, loc[a]] * np.prod([w[ax, loc[ax]] for ax in range(d) if ax != a])
+                g[a] += ga * v / self.spacing[a]
+                for b in range(d):
+                    if a == b:
+                        hab = d2[a, loc[a]] * np.prod([w[ax, loc[ax]] for ax in range(d) if ax != a])
+                    else:
+                        hab = d1[a, loc[a]] * d1[b, loc[b]] * np.prod(
+                            [w[ax, loc[ax]] for ax in range(d) if ax not in (a, b)])
+                    H[a, b] += hab * v / (self.spacing[a] * self.spacing[b])
+        return c, g, H
+
+    def __call__(self, x):
+        x = np.asarray(x, float)
+        flat = x.reshape(-1, x.shape[-1])
+        return np.asarray([self.eval(p)[0] for p in flat]).reshape(x.shape[:-1])
+
+
+class LinearSpeed:
+    """c(x) = a + b . x (the reference's analytic test media)."""
+
+    def __init__(self, a, b):
+        self.a = float(a)
+        self.b = np.asarray(b, float)
+
+    def eval(self, x):
+        d = self.b.size
+        return self.a + self.b @ np.asarray(x, float), self.b.copy(), np.zeros((d, d))
+
+
+def rhs(t, y, mode, speed, d, lam=0.0):
+    """coupled_rhs_absorption (gb/gb_solvers.py:820-867) on a real-packed state
+    y = [x (d), p (d), Re M (d^2), Im M (d^2), Re A, Im A]."""
+    x = y[:d]
+    p = y[d:2 * d]
+    M = (y[2 * d:2 * d + d * d] + 1j * y[2 * d + d * d:2 * d + 2 * d * d]).reshape(d, d)
+    A = y[-2] + 1j * y[-1]
+    c, gc, hc = speed.eval(x)
+    npn = np.linalg.norm(p)
+    G = mode * c * npn
+    Gx = mode * gc * npn
+    Gp = mode * c * p / npn
+    Gpp = mode * c * (np.eye(d) / npn - np.outer(p, p) / npn ** 3)
+    Gxp = mode * np.outer(gc, p) / npn
+    Gxx = mode * hc * npn
+    dM = -(Gxx + Gxp @ M + M @ Gxp.T + M @ Gpp @ M)
+    dA = -A * (c ** 2 * np.trace(M) - Gx @ Gp - Gp @ M @ Gp + lam * G) / (2 * G)
+    return np.concatenate([Gp, -Gx, dM.real.ravel(), dM.imag.ravel(), [dA.real, dA.imag]])
+
+
+def solve(x0, p0, M0, a0, mode, ts, speed, lam=0.0, rtol=1e-12, atol=1e-12):
+    """One beam with DOP853; returns xt (Nt, d), pt, Mt (Nt, d, d), At (Nt,)."""
+    d = len(x0)
+    M0 = np.asarray(M0, complex)
+    y0 = np.concatenate([x0, p0, M0.real.ravel(), M0.imag.ravel(), [np.real(a0), np.imag(a0)]])
+    ts = np.asarray(ts, float)
+    sol = solve_ivp(lambda t, y: rhs(t, y, mode, speed, d, lam), (ts[0], ts[-1]), y0, method="DOP853",
+                    rtol=rtol, atol=atol, t_eval=ts)
+    if not sol.success:
+        raise RuntimeError(sol.message)
+    Y = sol.y.T
+    xt = Y[:, :d]
+    pt = Y[:, d:2 * d]
+    Mt = (Y[:, 2 * d:2 * d + d * d] + 1j * Y[:, 2 * d + d * d:2 * d + 2 * d * d]).reshape(-1, d, d)
+    At = Y[:, -2] + 1j * Y[:, -1]
+    return xt, pt, Mt, At
+
+
+def analytic_1d_linear(x0, p0, M0, A0, ts, a, b):
+    """tests/test_gb.py:630-667: closed forms for c = a + b x, mode +1, p > 0."""
+    dt = np.asarray(ts) - ts[0]
+    return ((x0 + a / b) * np.exp(b * dt) - a / b, p0 * np.exp(-b * dt), M0 * np.exp(-2 * b * dt),
+            A0 * np.exp(0.5 * b * dt))
+
+
+def beam_field(xt, pt, Mt, At, omega, sensors, domain_size, periodic):
+    """Real field of one beam from its trajectory (gb/core.py:267-303), (Nt, Ns)."""
+    from .msgb import gaussian_beam_real_sum
+
+    return gaussian_beam_real_sum(xt[None], pt[None], Mt[None], At[None, :, None], np.array([omega]),
+                                  np.asarray(sensors), domain_size, periodic)
