@@ -52,6 +52,27 @@ class MswptDesc(ctypes.Structure):
                 ("lattice_offset", c_vp), ("lattice_box", c_vp)]
 
 
+class Medium(ctypes.Structure):
+    _fields_ = [("kind", c_i32), ("boundary", c_i32), ("n", c_i32 * 3), ("spacing", c_dbl * 3),
+                ("origin", c_dbl * 3), ("coeffs", c_vp), ("c", c_dbl), ("lam", c_dbl)]
+
+
+class OdeOpts(ctypes.Structure):
+    _fields_ = [("method", c_i32), ("substeps", c_i32), ("rtol", c_dbl), ("atol", c_dbl), ("dt0", c_dbl),
+                ("max_steps", c_i64)]
+
+
+class Trajectories(ctypes.Structure):
+    _fields_ = [("nb", c_i64), ("b_first", c_i64), ("rec64", c_vp), ("rec32", c_vp), ("cull", c_vp),
+                ("status", c_vp)]
+
+
+class Gemm(ctypes.Structure):
+    _fields_ = [("A", c_vp), ("sAm", c_i64), ("sAk", c_i64), ("B", c_vp), ("sBn", c_i64), ("sBk", c_i64),
+                ("M", c_i32), ("N", c_i32), ("K", c_i32), ("bias", c_vp), ("act", c_i32), ("C32", c_vp),
+                ("ldc32", c_i64), ("C16", c_vp), ("ldc16", c_i64), ("error_flag", c_vp)]
+
+
 class BeamOut(ctypes.Structure):
     _fields_ = [("x0", c_vp), ("p0", c_vp), ("alpha", c_vp), ("a0", c_vp), ("omega", c_vp),
                 ("a0_unit", c_vp)]
@@ -66,6 +87,19 @@ SIGNATURES = {
     "msgb_sum_f32_workspace_size": (c_sz, [c_vp, c_i64]),
     "msgb_sum_fwd_f32": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_sz, c_vp, c_vp]),
     "msgb_adj_gather_f32": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_sz, c_vp, c_vp, c_vp]),
+    "msgb_rk4_trajectories": (ctypes.c_int, [c_vp, c_vp, c_vp, ctypes.c_int, c_vp, c_vp]),
+    "msgb_ode_trajectories": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "msgb_sum_fwd_f64_traj": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "msgb_adj_gather_f64_traj": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "msgb_sum_f32_traj_workspace_size": (c_sz, [c_vp, c_i64]),
+    "msgb_sum_fwd_f32_traj": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, ctypes.c_int, ctypes.c_int, c_vp, c_sz,
+                                              c_vp, c_vp]),
+    "msgb_adj_gather_f32_traj": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_sz, c_vp, c_vp, c_vp]),
+    "msgb_gemm_bf16": (ctypes.c_int, [c_vp, c_vp]),
+    "msgb_silu_backward": (ctypes.c_int, [c_vp, c_vp, c_i64, c_vp, c_vp, c_vp]),
+    "msgb_colsum": (ctypes.c_int, [c_vp, ctypes.c_int, ctypes.c_int, c_i64, c_vp, c_vp]),
+    "msgb_adam": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_i64, c_dbl, c_dbl, c_dbl, c_dbl, c_i64, c_vp, c_vp]),
+    "msgb_to_bf16": (ctypes.c_int, [c_vp, c_i64, c_vp, c_vp]),
     "msgb_mswpt_create": (ctypes.c_int, [c_vp, c_vp]),
     "msgb_mswpt_destroy": (ctypes.c_int, [c_vp]),
     "msgb_mswpt_total_coeffs": (c_i64, [c_vp]),

@@ -1,6 +1,6 @@
-// Heterogeneous beam propagation: fixed-step FP64 RK4 for the ray, the
-// complex Hessian (Riccati) and the amplitude, in a sound speed interpolated
-// from a grid.
+// Heterogeneous beam propagation: FP64 integration of the ray, the complex
+// Hessian (Riccati) and the amplitude, in a sound speed interpolated from a
+// grid.
 //
 // Restates coupled_rhs_absorption (beamax gb/gb_solvers.py:820-867) and
 // riccati_rhs (:787-817):
@@ -10,10 +10,12 @@
 // with c, grad c and hess c of make_c_function_from_grid (utils/interp.py:
 // 31-263: n-linear or cubic B-spline tensor product, boundary maps
 // nearest/wrap/reflect/mirror), evaluated with analytic weight derivatives.
-// The reference integrates with adaptive Tsit5 (:706-784); here the step is
-// the acquisition step divided by `substeps`, one thread per beam, and the
-// state is written at every acquisition time.  A is integrated from 1 (the
-// equation is linear in A): the summation multiplies by the beam amplitude.
+// The reference integrates with adaptive Tsit5 under a PID step controller
+// (:706-784).  Here: adaptive Dormand-Prince 5(4) with the same tolerances,
+// error norm and step-count limit, or fixed-step RK4 (`substeps` equal steps
+// per save interval).  One thread per beam; the state is written at every
+// acquisition time.  A is integrated from 1 (the equation is linear in A):
+// the summation multiplies by the beam amplitude.
 #include "common.cuh"
 
 namespace msgb {
@@ -250,6 +252,120 @@ __device__ void rk4_step(const MediumArgs &med, double mode, State<D> &y, double
     y.A = y.A + h6 * (k1.A + 2.0 * k2.A + 2.0 * k3.A + k4.A);
 }
 
+// Dormand & Prince (1980) 5(4) pair.  Row s of DP_A gives stage s's input
+// y + h sum_j DP_A[s][j] k_j; the last row equals the 5th-order weights
+// (first same as last: k_7 = f(y_next) starts the next step).  DP_E = 5th- minus
+// 4th-order weights, the local error estimate.
+__constant__ double DP_A[7][6] = {
+    {0, 0, 0, 0, 0, 0},
+    {1.0 / 5, 0, 0, 0, 0, 0},
+    {3.0 / 40, 9.0 / 40, 0, 0, 0, 0},
+    {44.0 / 45, -56.0 / 15, 32.0 / 9, 0, 0, 0},
+    {19372.0 / 6561, -25360.0 / 2187, 64448.0 / 6561, -212.0 / 729, 0, 0},
+    {9017.0 / 3168, -355.0 / 33, 46732.0 / 5247, 49.0 / 176, -5103.0 / 18656, 0},
+    {35.0 / 384, 0, 500.0 / 1113, 125.0 / 192, -2187.0 / 6784, 11.0 / 84}};
+__constant__ double DP_E[7] = {35.0 / 384 - 5179.0 / 57600,
+                               0.0,
+                               500.0 / 1113 - 7571.0 / 16695,
+                               125.0 / 192 - 393.0 / 640,
+                               -2187.0 / 6784 + 92097.0 / 339200,
+                               11.0 / 84 - 187.0 / 2100,
+                               -1.0 / 40};
+
+struct OdeArgs {
+    int method, substeps;
+    double rtol, atol, dt0;
+    int64_t max_steps;
+};
+
+template <int D>
+struct NV {
+    static constexpr int value = 2 * D + 2 * D * D + 2;  // doubles in State<D>
+};
+
+template <int D>
+__device__ __forceinline__ double *vals(State<D> &s) { return reinterpret_cast<double *>(&s); }
+template <int D>
+__device__ __forceinline__ const double *vals(const State<D> &s) { return reinterpret_cast<const double *>(&s); }
+
+// Magnitude of complex entry e of the state (x and p entries are real).
+template <int D>
+__device__ __forceinline__ double entry_abs(const double *v, int e) {
+    if (e < 2 * D) return fabs(v[e]);
+    const int q = 2 * D + 2 * (e - 2 * D);
+    return hypot(v[q], v[q + 1]);
+}
+
+// One adaptive step attempt sequence from t to t_end.  Returns 0, or 2 when
+// the step budget runs out (the state then stays at the last accepted step).
+template <int D>
+__device__ int dopri_advance(const MediumArgs &med, double mode, State<D> &y, State<D> &f0, double &t,
+                             const double t_end, double &h, int64_t &steps, const OdeArgs &o) {
+    constexpr int N = NV<D>::value;
+    constexpr int NE = 2 * D + D * D + 1;
+    static_assert(sizeof(State<D>) == N * sizeof(double), "State<D> must be a plain array of doubles");
+    while (t < t_end) {
+        if (steps >= o.max_steps) return 2;
+        double hh = h;
+        bool clipped = false;
+        if (t + hh >= t_end) {
+            hh = t_end - t;
+            clipped = true;
+        }
+        State<D> k[7];
+        k[0] = f0;
+        State<D> yt;
+        const double *yv = vals(y);
+#pragma unroll 1
+        for (int s = 1; s < 7; ++s) {
+            double *tv = vals(yt);
+#pragma unroll
+            for (int c = 0; c < N; ++c) {
+                double acc = 0.0;
+                for (int j = 0; j < s; ++j) {
+                    const double a = DP_A[s][j];
+                    if (a != 0.0) acc += a * vals(k[j])[c];
+                }
+                tv[c] = yv[c] + hh * acc;
+            }
+            rhs<D>(med, mode, yt, k[s]);
+        }
+        // yt now holds the 5th-order solution (stage 7's input).
+        double ev[N];
+#pragma unroll
+        for (int c = 0; c < N; ++c) {
+            double acc = 0.0;
+            for (int j = 0; j < 7; ++j) acc += DP_E[j] * vals(k[j])[c];
+            ev[c] = hh * acc;
+        }
+        double sum = 0.0;
+        const double *nv = vals(yt);
+#pragma unroll
+        for (int e = 0; e < NE; ++e) {
+            const double sc = o.atol + o.rtol * fmax(entry_abs<D>(yv, e), entry_abs<D>(nv, e));
+            const double r = entry_abs<D>(ev, e) / sc;
+            sum += r * r;
+        }
+        const double err = sqrt(sum / NE);
+        ++steps;
+        if (!isfinite(err)) {
+            h = 0.2 * hh;
+            continue;
+        }
+        const double fac = err == 0.0 ? 10.0 : fmin(10.0, fmax(0.2, 0.9 * pow(err, -0.2)));
+        if (err <= 1.0) {
+            t = clipped ? t_end : t + hh;
+            y = yt;
+            f0 = k[6];
+            const double hn = hh * fac;
+            h = clipped ? fmax(hn, h) : hn;
+        } else {
+            h = hh * fmin(1.0, fac);
+        }
+    }
+    return 0;
+}
+
 // Smallest eigenvalue of a symmetric D x D matrix (exact for D <= 2,
 // Gershgorin lower bound for D = 3).
 template <int D>
@@ -281,10 +397,9 @@ struct TrajArgs {
 };
 
 template <int D>
-__global__ void rk4_kernel(ProbArgs P, MediumArgs med, BeamArgs B, TrajArgs T, int substeps, int tt_len) {
+__global__ void ode_kernel(ProbArgs P, MediumArgs med, BeamArgs B, TrajArgs T, OdeArgs o, int tt_len) {
     const int64_t bl = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (bl >= T.nb) return;
-    const double dt = P.nt > 1 ? P.ts[1] - P.ts[0] : 0.0;
     const int64_t b = T.b_first + bl;
     const int64_t j = b < B.n ? b : b - B.n;
     const double mode = b < B.n ? 1.0 : -1.0;
@@ -299,7 +414,13 @@ __global__ void rk4_kernel(ProbArgs P, MediumArgs med, BeamArgs B, TrajArgs T, i
     }
     y.A = cd{1.0, 0.0};
     const double w = B.omega[j];
-    const double h = dt / substeps;
+    const bool adaptive = o.method == MSGB_ODE_DOPRI5;
+    double h = o.dt0 > 0.0 ? o.dt0 : (P.nt > 1 ? P.ts[1] - P.ts[0] : 0.0);
+    double t = P.ts[0];
+    int64_t steps = 0;
+    int code = 0;
+    State<D> f0;
+    if (adaptive) rhs<D>(med, mode, y, f0);
     constexpr int S = D * (D + 1) / 2;
     constexpr int NR64 = 2 * D + 2 * D * D + 2;
     float lo[D], hi[D];
@@ -307,12 +428,19 @@ __global__ void rk4_kernel(ProbArgs P, MediumArgs med, BeamArgs B, TrajArgs T, i
     bool bad = false;
     const int64_t n_tt = (P.nt + tt_len - 1) / tt_len;
     for (int64_t k = 0; k < P.nt; ++k) {
-        if (k > 0)
-            for (int s = 0; s < substeps; ++s) rk4_step<D>(med, mode, y, h);
+        if (k > 0 && code == 0) {
+            if (adaptive) {
+                code = dopri_advance<D>(med, mode, y, f0, t, P.ts[k], h, steps, o);
+            } else {
+                const double hs = (P.ts[k] - P.ts[k - 1]) / o.substeps;
+                for (int s = 0; s < o.substeps; ++s) rk4_step<D>(med, mode, y, hs);
+            }
+        }
         bool fin = isfinite(y.A.re) && isfinite(y.A.im);
 #pragma unroll
         for (int i = 0; i < D; ++i) fin = fin && isfinite(y.x[i]) && isfinite(y.p[i]);
-        bad |= !fin;
+        if (!fin && code == 0) code = 1;
+        bad |= code != 0;
         double xw[D];
 #pragma unroll
         for (int i = 0; i < D; ++i) xw[i] = P.periodic[i] ? pymod(y.x[i], P.L[i]) : y.x[i];
@@ -391,7 +519,7 @@ __global__ void rk4_kernel(ProbArgs P, MediumArgs med, BeamArgs B, TrajArgs T, i
         }
     }
     (void)n_tt;
-    if (T.status) T.status[bl] = bad ? 1 : 0;
+    if (T.status) T.status[bl] = code;
 }
 
 }  // namespace
@@ -399,12 +527,22 @@ __global__ void rk4_kernel(ProbArgs P, MediumArgs med, BeamArgs B, TrajArgs T, i
 
 using namespace msgb;
 
-extern "C" int msgb_rk4_trajectories(const msgb_problem *prob, const msgb_medium *med, const msgb_beam_set *beams,
-                                     int substeps, const msgb_trajectories *out, msgb_stream_t stream) {
+extern "C" int msgb_ode_trajectories(const msgb_problem *prob, const msgb_medium *med, const msgb_beam_set *beams,
+                                     const msgb_ode_opts *opts, const msgb_trajectories *out,
+                                     msgb_stream_t stream) {
     if (int e = validate_problem(prob)) return e;
     if (int e = validate_beams(prob, beams)) return e;
-    if (!med || !out) return fail(MSGB_ERR_ARG, "msgb_rk4_trajectories: NULL medium or output");
-    if (substeps < 1) return fail(MSGB_ERR_ARG, "substeps must be >= 1");
+    if (!med || !out || !opts) return fail(MSGB_ERR_ARG, "msgb_ode_trajectories: NULL medium, options or output");
+    if (opts->method == MSGB_ODE_RK4) {
+        if (opts->substeps < 1) return fail(MSGB_ERR_ARG, "substeps must be >= 1");
+    } else if (opts->method == MSGB_ODE_DOPRI5) {
+        if (!(opts->rtol > 0.0) || !(opts->atol > 0.0) || !isfinite(opts->rtol) || !isfinite(opts->atol))
+            return fail(MSGB_ERR_ARG, "rtol and atol must be finite and positive");
+        if (opts->max_steps < 1) return fail(MSGB_ERR_ARG, "max_steps must be a positive integer");
+        if (!isfinite(opts->dt0)) return fail(MSGB_ERR_ARG, "dt0 must be finite");
+    } else {
+        return fail(MSGB_ERR_ARG, "unknown ODE method %d", opts->method);
+    }
     if (out->nb < 0 || out->b_first < 0 || out->b_first + out->nb > 2 * beams->n)
         return fail(MSGB_ERR_ARG, "beam range [%lld, %lld) outside [0, 2n)", (long long)out->b_first,
                     (long long)(out->b_first + out->nb));
@@ -431,14 +569,23 @@ extern "C" int msgb_rk4_trajectories(const msgb_problem *prob, const msgb_medium
     M.coeffs = med->coeffs;
     M.c = med->c;
     M.lam = med->lam;
+    OdeArgs O{opts->method, opts->substeps, opts->rtol, opts->atol, opts->dt0, opts->max_steps};
     TrajArgs T{out->nb, out->b_first, beams->n, out->rec64, out->rec32, out->cull, out->status};
-    const int blk = 128;
+    const int blk = 64;
     const unsigned grid = (unsigned)((out->nb + blk - 1) / blk);
     cudaStream_t st = as_stream(stream);
     switch (prob->ndim) {
-        case 1: rk4_kernel<1><<<grid, blk, 0, st>>>(P, M, to_args(beams), T, substeps, MSGB_TIME_TILE); break;
-        case 2: rk4_kernel<2><<<grid, blk, 0, st>>>(P, M, to_args(beams), T, substeps, MSGB_TIME_TILE); break;
-        default: rk4_kernel<3><<<grid, blk, 0, st>>>(P, M, to_args(beams), T, substeps, MSGB_TIME_TILE); break;
+        case 1: ode_kernel<1><<<grid, blk, 0, st>>>(P, M, to_args(beams), T, O, MSGB_TIME_TILE); break;
+        case 2: ode_kernel<2><<<grid, blk, 0, st>>>(P, M, to_args(beams), T, O, MSGB_TIME_TILE); break;
+        default: ode_kernel<3><<<grid, blk, 0, st>>>(P, M, to_args(beams), T, O, MSGB_TIME_TILE); break;
     }
-    return check_launch("msgb_rk4_trajectories");
+    return check_launch("msgb_ode_trajectories");
+}
+
+extern "C" int msgb_rk4_trajectories(const msgb_problem *prob, const msgb_medium *med, const msgb_beam_set *beams,
+                                     int substeps, const msgb_trajectories *out, msgb_stream_t stream) {
+    msgb_ode_opts o{};
+    o.method = MSGB_ODE_RK4;
+    o.substeps = substeps;
+    return msgb_ode_trajectories(prob, med, beams, &o, out, stream);
 }

@@ -258,11 +258,20 @@ __device__ __forceinline__ void anchor(const ProbArgs &P, const BeamTime<D> &bt,
     r.amp = bt.amp;
 }
 
+// Largest e-fold count the run recurrence may meet: at the seed (chi), in the
+// first step's ratio and in the ratio's own step.  Beyond it the factors leave
+// FP32's range (e^88) and the recurrence would produce 0 * inf; such runs are
+// evaluated directly.  Only very narrow beams (e-fold width under about one
+// sensor spacing over a 16-sensor run, e.g. after focusing in a
+// heterogeneous medium) reach it.
+constexpr float kRecurrenceEfolds = 60.0f;
+
 // Direct evaluation at a run start (seed): z, and the recurrence factors for
-// the step h to the next sensor.
+// the step h to the next sensor.  With `safe`, reports whether the recurrence
+// stays within kRecurrenceEfolds.
 template <int D, bool PERIODIC>
 __device__ __forceinline__ cf seed_eval(const Rec<D> &r, const float *ds, const float *h, bool cont,
-                                        const ProbArgs &P, cf &rr, cf &qq) {
+                                        const ProbArgs &P, cf &rr, cf &qq, bool *safe = nullptr) {
     float Dl[D];
     float th = r.th0;
 #pragma unroll
@@ -284,6 +293,8 @@ __device__ __forceinline__ cf seed_eval(const Rec<D> &r, const float *ds, const 
         const float a2r = -quad<D>(r.p, h), a2i = quad<D>(r.q, h);
         rr = cexpf_(a1r + a2r, a1i + a2i);
         qq = cexpf_(2.0f * a2r, 2.0f * a2i);
+        if (safe)
+            *safe = chi <= kRecurrenceEfolds && a1r + a2r <= kRecurrenceEfolds && -2.0f * a2r <= kRecurrenceEfolds;
     }
     return z;
 }
@@ -455,6 +466,43 @@ __global__ void transpose_permute_kernel(const float *data, const int32_t *perm,
     }
 }
 
+// ------------------------------------------------------------------ trajectories
+// Records written by msgb_rk4_trajectories (rec32) for a chunk of beams, the
+// per-time-tile culling boxes, and the Kahan state carried across chunks.
+template <int D>
+struct TrajSrc {
+    int64_t nb, b_first;
+    const BeamTime<D> *rec;   // (nt, nb)
+    const float *cull;        // (n_tt, nb, 2D + 1)
+    float *state;             // (2, nt, ns) Kahan sum / compensation, sorted sensor order
+    int first, last;
+};
+
+template <int D>
+__device__ __forceinline__ bool traj_survives(const TrajSrc<D> &T, int64_t bl, int64_t tt, const TileInfo<D> &ti,
+                                              float cutoff) {
+    if (cutoff <= 0.0f) return true;
+    const float *c = T.cull + (tt * T.nb + bl) * (2 * D + 1);
+    float d2 = 0.0f;
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+        const float gap = fmaxf(0.0f, fmaxf(ti.lo[i] - c[D + i], c[i] - ti.hi[i]));
+        d2 = fmaf(gap, gap, d2);
+    }
+    return c[2 * D] * d2 * 0.999f <= cutoff;
+}
+
+template <int D>
+__device__ __forceinline__ void traj_beam_time(const BeamArgs &B, const TrajSrc<D> &T, int64_t bl, int64_t k,
+                                               BeamTime<D> &bt) {
+    bt = T.rec[k * T.nb + bl];
+    const int64_t b = T.b_first + bl;
+    const int64_t j = b < B.n ? b : b - B.n;
+    const double ar = B.a0[2 * j], ai = B.a0[2 * j + 1];
+    bt.amp = (float)((double)bt.amp * hypot(ar, ai));
+    bt.ang = (float)((double)bt.ang + atan2(ai, (ar == 0.0 && ai == 0.0) ? 1e-12 : ar));
+}
+
 // ------------------------------------------------------------------ forward
 template <int D>
 __device__ __forceinline__ void load_rec(const float (*rec)[G][TT], int gl, int lane, Rec<D> &r) {
@@ -473,12 +521,12 @@ __device__ __forceinline__ void kahan_add(float &acc, float &cmp, float v) {
 // Persistent CTAs take (time tile, sensor tile) work items from a counter.
 // Warp w owns sensor group w (GS sensors) of the tile; lane l owns time l.
 // Beams are evaluated two at a time (independent recurrence chains).
-template <int D, bool PERIODIC>
+template <int D, bool PERIODIC, bool TRAJ>
 __global__ void __launch_bounds__(THREADS, 2)
 fwd32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *tiles, const int32_t *offs,
              const float *ds_g, const float *hn_g, const uint8_t *seed_g, const uint8_t *gfast_g,
              const int32_t *perm, float cutoff, float *out, unsigned long long *eval_count, int *work, int n_st,
-             int n_tiles) {
+             int n_tiles, TrajSrc<D> T) {
     constexpr int NF = Rec<D>::NF;
     __shared__ float rec[NF][G][TT];
     __shared__ float sds[TS][D], shn[TS][D];
@@ -515,14 +563,30 @@ fwd32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
         float acc[GS], cmp[GS];
 #pragma unroll
         for (int k = 0; k < GS; ++k) acc[k] = 0.0f, cmp[k] = 0.0f;
+        if (TRAJ && !T.first && lane < t_cnt && active) {
+            const int64_t t = t_first + lane;
+#pragma unroll
+            for (int k = 0; k < GS; ++k) {
+                const int s = gbase + k;
+                if (s < s_cnt) {
+                    acc[k] = T.state[t * P.ns + s_first + s];
+                    cmp[k] = T.state[(P.nt + t) * P.ns + s_first + s];
+                }
+            }
+        }
+        const int64_t nbeam = TRAJ ? T.nb : B.n;
 
-        for (int64_t j0 = 0; j0 < B.n; j0 += THREADS) {
+        for (int64_t j0 = 0; j0 < nbeam; j0 += THREADS) {
             const int64_t j = j0 + tid;
             bool keep_p = false, keep_m = false;
-            if (j < B.n) {
-                const Cull<D> cb = cull[j];
-                keep_p = survives<D>(cb, (float)P.c, ta, tb, ti, P, cutoff);
-                keep_m = survives<D>(cb, -(float)P.c, ta, tb, ti, P, cutoff);
+            if (j < nbeam) {
+                if (TRAJ) {
+                    keep_p = traj_survives<D>(T, j, tt, ti, cutoff);
+                } else {
+                    const Cull<D> cb = cull[j];
+                    keep_p = survives<D>(cb, (float)P.c, ta, tb, ti, P, cutoff);
+                    keep_m = survives<D>(cb, -(float)P.c, ta, tb, ti, P, cutoff);
+                }
             }
             const unsigned bp = __ballot_sync(0xffffffffu, keep_p);
             const unsigned bm = __ballot_sync(0xffffffffu, keep_m);
@@ -547,7 +611,10 @@ fwd32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
                     Rec<D> r;
                     if (g0 + gl < nsurv && tloc < t_cnt) {
                         BeamTime<D> bt;
-                        beam_time<D>(P, B, surv[g0 + gl], P.ts[t_first + tloc], bt);
+                        if (TRAJ)
+                            traj_beam_time<D>(B, T, surv[g0 + gl], t_first + tloc, bt);
+                        else
+                            beam_time<D>(P, B, surv[g0 + gl], P.ts[t_first + tloc], bt);
                         anchor<D>(P, bt, ti.s0, r);
                     } else {
 #pragma unroll
@@ -568,10 +635,13 @@ fwd32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
                         Rec<D> ra, rb;
                         load_rec<D>(rec, gl, lane, ra);
                         load_rec<D>(rec, gl + 1, lane, rb);  // zero-amplitude record when gl + 1 == ng
+                        cf za, fa, qa, zb, fb, qb;
+                        bool oka = true, okb = true;
                         if (fast) {
-                            cf za, fa, qa, zb, fb, qb;
-                            za = seed_eval<D, false>(ra, sds[gbase], shn[gbase], true, P, fa, qa);
-                            zb = seed_eval<D, false>(rb, sds[gbase], shn[gbase], true, P, fb, qb);
+                            za = seed_eval<D, false>(ra, sds[gbase], shn[gbase], true, P, fa, qa, &oka);
+                            zb = seed_eval<D, false>(rb, sds[gbase], shn[gbase], true, P, fb, qb, &okb);
+                        }
+                        if (fast && oka && okb) {
                             kahan_add(acc[0], cmp[0], za.re + zb.re);
 #pragma unroll
                             for (int k = 1; k < GS; ++k) {
@@ -601,7 +671,14 @@ fwd32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
 #pragma unroll
             for (int k = 0; k < GS; ++k) {
                 const int s = gbase + k;
-                if (s < s_cnt) out[t * P.ns + perm[s_first + s]] = acc[k] - cmp[k];
+                if (s < s_cnt) {
+                    if (TRAJ && !T.last) {
+                        T.state[t * P.ns + s_first + s] = acc[k];
+                        T.state[(P.nt + t) * P.ns + s_first + s] = cmp[k];
+                    } else {
+                        out[t * P.ns + perm[s_first + s]] = acc[k] - cmp[k];
+                    }
+                }
             }
         }
         __syncthreads();
@@ -618,20 +695,20 @@ fwd32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
 // direct evaluation.  Data is in sorted-sensor-major layout (lanes read
 // consecutive times).  Per-tile FP32 partials go into FP64; the warp result is
 // reduced in a fixed order, so the output is deterministic.
-template <int D, bool PERIODIC>
+template <int D, bool PERIODIC, bool TRAJ>
 __global__ void __launch_bounds__(THREADS)
 adj32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *tiles, const int32_t *offs,
              int64_t n_st, const float *ds_g, const float *hn_g, const uint8_t *gfast_g, const float *dataT,
-             float cutoff, double *g, unsigned long long *eval_count) {
+             float cutoff, double *g, unsigned long long *eval_count, TrajSrc<D> T) {
     constexpr int CH = 4;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t j = (int64_t)blockIdx.x * NW + warp;
-    if (j >= B.n) return;
-    const Cull<D> cb = cull[j];
+    if (j >= (TRAJ ? T.nb : B.n)) return;
+    const Cull<D> cb = TRAJ ? Cull<D>{} : cull[j];
     const int64_t n_tt = (P.nt + TT - 1) / TT;
     double gre = 0.0, gim = 0.0;
     unsigned long long evals = 0;
-    for (int m = 0; m < 2; ++m) {
+    for (int m = 0; m < (TRAJ ? 1 : 2); ++m) {
         const float c0 = m == 0 ? (float)P.c : -(float)P.c;
         const int64_t b = m == 0 ? j : j + B.n;
         for (int64_t tt = 0; tt < n_tt; ++tt) {
@@ -644,10 +721,16 @@ adj32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
             BeamTime<D> bt;
             for (int64_t st0 = 0; st0 < n_st; st0 += 32) {
                 const int64_t st_l = st0 + lane;
-                const bool keep = st_l < n_st && survives<D>(cb, c0, ta, tb, tiles[st_l], P, cutoff);
+                bool keep = false;
+                if (st_l < n_st)
+                    keep = TRAJ ? traj_survives<D>(T, j, tt, tiles[st_l], cutoff)
+                                : survives<D>(cb, c0, ta, tb, tiles[st_l], P, cutoff);
                 unsigned mask = __ballot_sync(0xffffffffu, keep);
                 if (mask && !have_bt) {
-                    beam_time<D>(P, B, b, P.ts[t], bt);
+                    if (TRAJ)
+                        traj_beam_time<D>(B, T, j, t, bt);
+                    else
+                        beam_time<D>(P, B, b, P.ts[t], bt);
                     have_bt = true;
                 }
                 while (mask) {
@@ -670,6 +753,7 @@ adj32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
                         if (gq + CH <= ngroups && ((fastbits >> gq) & ((1u << CH) - 1u)) == ((1u << CH) - 1u)) {
                             cf z[CH], rr[CH], qq[CH];
                             float d[CH];
+                            bool ok = true;
 #pragma unroll
                             for (int c = 0; c < CH; ++c) {
                                 const int s = (gq + c) * GS;
@@ -677,8 +761,26 @@ adj32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
 #pragma unroll
                                 for (int i = 0; i < D; ++i)
                                     dsl[i] = __ldg(ds_g + (s_first + s) * D + i), hl[i] = __ldg(hn_g + (s_first + s) * D + i);
-                                z[c] = seed_eval<D, false>(r, dsl, hl, true, P, rr[c], qq[c]);
+                                bool okc = true;
+                                z[c] = seed_eval<D, false>(r, dsl, hl, true, P, rr[c], qq[c], &okc);
+                                ok = ok && okc;
                                 d[c] = tv ? __ldg(dcol + (int64_t)s * P.nt) : 0.0f;
+                            }
+                            if (!ok) {
+                                // out-of-range recurrence: these CH groups sensor by sensor
+                                for (int s = gq * GS; s < (gq + CH) * GS; ++s) {
+                                    float dsl[D], hl[D];
+#pragma unroll
+                                    for (int i = 0; i < D; ++i)
+                                        dsl[i] = __ldg(ds_g + (s_first + s) * D + i), hl[i] = 0.0f;
+                                    cf dr, dq;
+                                    const cf zd = seed_eval<D, false>(r, dsl, hl, false, P, dr, dq);
+                                    const float dd = tv ? __ldg(dcol + (int64_t)s * P.nt) : 0.0f;
+                                    pr = fmaf(dd, zd.re, pr);
+                                    pi = fmaf(-dd, zd.im, pi);
+                                }
+                                gq += CH;
+                                continue;
                             }
                             for (int kk = 0; kk < GS; ++kk) {
                                 float dn[CH];
@@ -843,9 +945,9 @@ int sm_count() {
     return n;
 }
 
-template <int D>
+template <int D, bool TRAJ>
 int run_fwd(const msgb_problem *p, const msgb_beam_set *b, const msgb_sum_opts *o, char *ws, const Layout &l,
-            float *out, cudaStream_t st) {
+            float *out, cudaStream_t st, TrajSrc<D> T) {
     if (int e = prep<D>(p, b, o, l, ws, st)) return e;
     const int64_t n_st = l.n_st, n_tt = (p->nt + TT - 1) / TT;
     if (n_st * n_tt > 0x7fffffffLL) return fail(MSGB_ERR_UNSUPPORTED, "msgb_sum_fwd_f32: too many tiles");
@@ -864,18 +966,18 @@ int run_fwd(const msgb_problem *p, const msgb_beam_set *b, const msgb_sum_opts *
                                        (const float *)(ws + l.hn), (const uint8_t *)(ws + l.seed),
                                        (const uint8_t *)(ws + l.gfast), (const int32_t *)(ws + l.vals_out),
                                        o ? (float)o->cutoff : 0.0f, out, o ? o->eval_count : nullptr, work,
-                                       (int)n_st, n_tiles);
+                                       (int)n_st, n_tiles, T);
     };
     if (periodic)
-        args(fwd32_kernel<D, true>);
+        args(fwd32_kernel<D, true, TRAJ>);
     else
-        args(fwd32_kernel<D, false>);
+        args(fwd32_kernel<D, false, TRAJ>);
     return check_launch("msgb_sum_fwd_f32");
 }
 
-template <int D>
+template <int D, bool TRAJ>
 int run_adj(const msgb_problem *p, const msgb_beam_set *b, const msgb_sum_opts *o, char *ws, const Layout &l,
-            const float *data, double *g, cudaStream_t st) {
+            const float *data, double *g, cudaStream_t st, TrajSrc<D> T) {
     if (int e = prep<D>(p, b, o, l, ws, st)) return e;
     dim3 tg((unsigned)((p->ns + 31) / 32), (unsigned)((p->nt + 31) / 32));
     if (tg.y > 65535u) return fail(MSGB_ERR_UNSUPPORTED, "msgb_adj_gather_f32: nt too large");
@@ -885,19 +987,35 @@ int run_adj(const msgb_problem *p, const msgb_beam_set *b, const msgb_sum_opts *
     P.sensors = (const double *)(ws + l.sorted);
     bool periodic = false;
     for (int i = 0; i < D; ++i) periodic |= (p->periodic[i] != 0);
-    const unsigned grid = (unsigned)((b->n + NW - 1) / NW);
+    const int64_t nw = TRAJ ? T.nb : b->n;
+    const unsigned grid = (unsigned)((nw + NW - 1) / NW);
     auto args = [&](auto kern) {
         kern<<<grid, THREADS, 0, st>>>(P, to_args(b), (const Cull<D> *)(ws + l.cull), (const TileInfo<D> *)(ws + l.tiles),
                                        (const int32_t *)(ws + l.offs), l.n_st, (const float *)(ws + l.ds),
                                        (const float *)(ws + l.hn), (const uint8_t *)(ws + l.gfast),
                                        (const float *)(ws + l.data), o ? (float)o->cutoff : 0.0f, g,
-                                       o ? o->eval_count : nullptr);
+                                       o ? o->eval_count : nullptr, T);
     };
     if (periodic)
-        args(adj32_kernel<D, true>);
+        args(adj32_kernel<D, true, TRAJ>);
     else
-        args(adj32_kernel<D, false>);
+        args(adj32_kernel<D, false, TRAJ>);
     return check_launch("msgb_adj_gather_f32");
+}
+
+template <int D>
+TrajSrc<D> traj_src(const msgb_trajectories *t, float *state, int first, int last) {
+    TrajSrc<D> T{};
+    if (t) {
+        T.nb = t->nb;
+        T.b_first = t->b_first;
+        T.rec = (const BeamTime<D> *)t->rec32;
+        T.cull = t->cull;
+    }
+    T.state = state;
+    T.first = first;
+    T.last = last;
+    return T;
 }
 
 }  // namespace
@@ -936,9 +1054,9 @@ extern "C" int msgb_sum_fwd_f32(const msgb_problem *prob, const msgb_beam_set *b
     cudaStream_t st = as_stream(stream);
     char *ws = (char *)workspace;
     switch (prob->ndim) {
-        case 1: return run_fwd<1>(prob, beams, opts, ws, l, out, st);
-        case 2: return run_fwd<2>(prob, beams, opts, ws, l, out, st);
-        default: return run_fwd<3>(prob, beams, opts, ws, l, out, st);
+        case 1: return run_fwd<1, false>(prob, beams, opts, ws, l, out, st, traj_src<1>(nullptr, nullptr, 1, 1));
+        case 2: return run_fwd<2, false>(prob, beams, opts, ws, l, out, st, traj_src<2>(nullptr, nullptr, 1, 1));
+        default: return run_fwd<3, false>(prob, beams, opts, ws, l, out, st, traj_src<3>(nullptr, nullptr, 1, 1));
     }
 }
 
@@ -958,8 +1076,75 @@ extern "C" int msgb_adj_gather_f32(const msgb_problem *prob, const msgb_beam_set
     cudaStream_t st = as_stream(stream);
     char *ws = (char *)workspace;
     switch (prob->ndim) {
-        case 1: return run_adj<1>(prob, beams, opts, ws, l, data, g, st);
-        case 2: return run_adj<2>(prob, beams, opts, ws, l, data, g, st);
-        default: return run_adj<3>(prob, beams, opts, ws, l, data, g, st);
+        case 1: return run_adj<1, false>(prob, beams, opts, ws, l, data, g, st, traj_src<1>(nullptr, nullptr, 1, 1));
+        case 2: return run_adj<2, false>(prob, beams, opts, ws, l, data, g, st, traj_src<2>(nullptr, nullptr, 1, 1));
+        default: return run_adj<3, false>(prob, beams, opts, ws, l, data, g, st, traj_src<3>(nullptr, nullptr, 1, 1));
     }
 }
+
+// ---- trajectory entry points ------------------------------------------------
+static size_t traj_state_offset(const Layout &l) { return l.total; }
+
+extern "C" size_t msgb_sum_f32_traj_workspace_size(const msgb_problem *prob, int64_t nb_max) {
+    if (validate_problem(prob) || nb_max < 0) return 0;
+    const Layout l = layout(prob, 0, true, (prob->ns + GS - 1) / GS);
+    return l.total + align256((size_t)2 * prob->nt * prob->ns * sizeof(float));
+}
+
+static int check_traj32(const msgb_problem *p, const msgb_beam_set *b, const msgb_trajectories *t,
+                        const msgb_sum_opts *o, void *ws, size_t bytes, Layout &l) {
+    if (!t || !t->rec32) return fail(MSGB_ERR_ARG, "FP32 trajectory records are NULL");
+    if (!t->cull && o && o->cutoff > 0.0) return fail(MSGB_ERR_ARG, "culling boxes are NULL");
+    if (t->nb < 0 || t->b_first < 0 || t->b_first + t->nb > 2 * b->n)
+        return fail(MSGB_ERR_ARG, "trajectory beam range outside [0, 2n)");
+    l = layout(p, 0, true, tile_count(p, o));
+    if (l.n_st <= 0) return fail(MSGB_ERR_ARG, "sensor tiling has no tiles");
+    const size_t need = l.total + align256((size_t)2 * p->nt * p->ns * sizeof(float));
+    if (!ws || bytes < need) return fail(MSGB_ERR_WORKSPACE, "workspace too small: need %zu bytes, got %zu", need, bytes);
+    if (((uintptr_t)ws & 255) != 0) return fail(MSGB_ERR_WORKSPACE, "workspace must be 256-byte aligned");
+    return MSGB_OK;
+}
+
+extern "C" int msgb_sum_fwd_f32_traj(const msgb_problem *prob, const msgb_beam_set *beams,
+                                     const msgb_trajectories *traj, const msgb_sum_opts *opts, int first_chunk,
+                                     int last_chunk, void *workspace, size_t workspace_bytes, float *out,
+                                     msgb_stream_t stream) {
+    if (int e = validate_problem(prob)) return e;
+    if (int e = validate_beams(prob, beams)) return e;
+    if (!out) return fail(MSGB_ERR_ARG, "msgb_sum_fwd_f32_traj: out is NULL");
+    if (prob->nt == 0 || prob->ns == 0) return MSGB_OK;
+    Layout l;
+    if (int e = check_traj32(prob, beams, traj, opts, workspace, workspace_bytes, l)) return e;
+    cudaStream_t st = as_stream(stream);
+    char *ws = (char *)workspace;
+    float *state = (float *)(ws + traj_state_offset(l));
+    const int f = first_chunk != 0, la = last_chunk != 0;
+    switch (prob->ndim) {
+        case 1: return run_fwd<1, true>(prob, beams, opts, ws, l, out, st, traj_src<1>(traj, state, f, la));
+        case 2: return run_fwd<2, true>(prob, beams, opts, ws, l, out, st, traj_src<2>(traj, state, f, la));
+        default: return run_fwd<3, true>(prob, beams, opts, ws, l, out, st, traj_src<3>(traj, state, f, la));
+    }
+}
+
+extern "C" int msgb_adj_gather_f32_traj(const msgb_problem *prob, const msgb_beam_set *beams,
+                                        const msgb_trajectories *traj, const msgb_sum_opts *opts, void *workspace,
+                                        size_t workspace_bytes, const float *data, double *g, msgb_stream_t stream) {
+    if (int e = validate_problem(prob)) return e;
+    if (int e = validate_beams(prob, beams)) return e;
+    if (!data || !g) return fail(MSGB_ERR_ARG, "msgb_adj_gather_f32_traj: NULL data or g");
+    if (!traj || traj->nb == 0) return MSGB_OK;
+    if (prob->nt == 0 || prob->ns == 0) {
+        cudaMemsetAsync(g, 0, sizeof(double) * 2 * traj->nb, as_stream(stream));
+        return check_launch("msgb_adj_gather_f32_traj");
+    }
+    Layout l;
+    if (int e = check_traj32(prob, beams, traj, opts, workspace, workspace_bytes, l)) return e;
+    cudaStream_t st = as_stream(stream);
+    char *ws = (char *)workspace;
+    switch (prob->ndim) {
+        case 1: return run_adj<1, true>(prob, beams, opts, ws, l, data, g, st, traj_src<1>(traj, nullptr, 1, 1));
+        case 2: return run_adj<2, true>(prob, beams, opts, ws, l, data, g, st, traj_src<2>(traj, nullptr, 1, 1));
+        default: return run_adj<3, true>(prob, beams, opts, ws, l, data, g, st, traj_src<3>(traj, nullptr, 1, 1));
+    }
+}
+

@@ -130,6 +130,29 @@ class Domain:
         tmax = self.xmax / self.compute_min_speed()
         return np.arange(0, tmax, dt)
 
+    def medium(self):
+        """The sound speed as the GPU propagator sees it.
+
+        Returns ``("constant", c)`` for a homogeneous medium and
+        ``("grid", interpolant)`` for a grid-valued speed (n-linear, wrap
+        boundary when every axis is periodic, clamp otherwise, as
+        geometry.py:191-203) or a ``GridInterpolant``.  Other callables are
+        only supported when they are constant on the grid.
+        """
+        from .utils.interp import GridInterpolant, make_c_function_from_grid
+
+        c = self.constant_speed()
+        if c is not None:
+            return "constant", c
+        if isinstance(self.c, GridInterpolant):
+            return "grid", self.c
+        if not callable(self.c):
+            return "grid", make_c_function_from_grid(np.asarray(self.c, float), spacing=self.dx,
+                                                     origin=(0.0,) * self.ndim,
+                                                     boundary="wrap" if all(self.periodic) else "clamp")
+        raise NotImplementedError("a non-constant Python callable c(x) cannot be evaluated on the GPU; "
+                                  "use utils.interp.make_c_function_from_grid")
+
     def constant_speed(self) -> Optional[float]:
         """The sound speed when the medium is homogeneous, else ``None``."""
         if callable(self.c):

@@ -34,7 +34,7 @@ import numpy as np
 from .. import _lib
 from .._device import DeviceCache, as_device_f64, default_device, workspace
 from ..geometry import Domain, Sensor
-from ..gb.gb_solvers import solver_name
+from ..gb.gb_solvers import SolverConfig, solver_name
 from ..transforms import MSWPT
 
 _cache = DeviceCache()
@@ -96,11 +96,16 @@ class MSGBSolver:
         evaluation, Kahan-compensated sums, FP64 anchor phases, Gaussian cutoff).
       cutoff: e-folds of the Gaussian envelope beyond which the FP32 path skips
         a (beam, time tile, sensor tile) triple.
+      rk4_substeps: RK4 steps per save interval when ``ode_config.solver`` is
+        "rk4" (overrides ``ode_config.substeps`` when > 1).
+      trajectory_memory: bytes of device memory for trajectory records; beams
+        are propagated and summed in chunks that fit.
     """
 
     def __init__(self, thr, thr_strat: str, batch_size: int, input_type: str, ode_solver, sum_method: str,
                  tr_ode_solver=None, sharding=None, ode_config=None, adjoint_relative_guard: float = 5e-2,
-                 *, precision: str = "fp64", cutoff: float = 16.0):
+                 *, precision: str = "fp64", cutoff: float = 16.0, rk4_substeps: int = 1,
+                 trajectory_memory: int = 16 << 30):
         valid_thresholds = {"hard", "top_n", "percentile", "hard_reassign", "bao_energy", "perc_max_abs"}
         if thr_strat not in valid_thresholds:
             raise ValueError(f"thr_strat must be one of {', '.join(sorted(valid_thresholds))}; got {thr_strat!r}.")
@@ -143,6 +148,10 @@ class MSGBSolver:
         self.ode_solver_name = solver_name(ode_solver)
         self.tr_ode_solver = ode_solver if tr_ode_solver is None else tr_ode_solver
         self.sharding = sharding
+        if ode_config is None:
+            ode_config = SolverConfig.from_precision()
+        if not isinstance(ode_config, SolverConfig):
+            raise TypeError("ode_config must be a beamax_b200.gb.gb_solvers.SolverConfig")
         self.ode_config = ode_config
         self.adjoint_relative_guard = float(adjoint_relative_guard)
         self.use_real = "real" in sum_method
@@ -150,6 +159,10 @@ class MSGBSolver:
         self.sum_method = sum_method
         self.precision = precision
         self.cutoff = float(cutoff)
+        if int(rk4_substeps) < 1:
+            raise ValueError("rk4_substeps must be a positive integer.")
+        self.rk4_substeps = max(int(rk4_substeps), ode_config.substeps)
+        self.trajectory_memory = int(trajectory_memory)
         self.last_selection: Optional[Selection] = None
         self.last_eval_count: Optional[int] = None
 
@@ -176,9 +189,9 @@ class MSGBSolver:
 
         c = domain.constant_speed()
         if c is None:
-            raise NotImplementedError("heterogeneous sound speed needs the RK4 beam path")
-        if domain.lam != 0.0:
-            raise NotImplementedError("absorption (lam != 0) is not supported by the summation kernels")
+            c = domain.compute_max_speed()  # unused by the trajectory kernels
+        elif domain.lam != 0.0:
+            raise NotImplementedError("absorption (lam != 0) needs the ODE path (heterogeneous media)")
         pos = np.ascontiguousarray(self._sensor_positions(sensors), np.float64)
         if pos.ndim != 2 or pos.shape[1] != domain.ndim:
             raise ValueError(f"sensor positions must have shape (Ns, {domain.ndim})")
@@ -274,9 +287,156 @@ class MSGBSolver:
                    "msgb_beam_init")
         return BeamTensors(x0, p0, al, a0, a0u, om)
 
+    # ------------------------------------------------------------- heterogeneous
+    def _medium(self, domain: Domain, device):
+        import torch
+
+        from ..utils.interp import BOUNDARY_CODE
+
+        kind, m = domain.medium()
+        med = _lib.Medium()
+        med.lam = float(domain.lam)
+        if kind == "constant":
+            med.kind = 0
+            med.c = float(m)
+            return med, None
+        med.kind = 1 if m.method == "linear" else 2
+        med.boundary = BOUNDARY_CODE[m.boundary]
+        for a in range(3):
+            med.n[a] = m.coeffs.shape[a] if a < m.ndim else 1
+            med.spacing[a] = float(m.spacing[a]) if a < m.ndim else 1.0
+            med.origin[a] = float(m.origin[a]) if a < m.ndim else 0.0
+        coeffs = _cache.get(m, ("coeffs", str(device)), lambda: torch.from_numpy(m.coeffs).to(device))
+        med.coeffs = coeffs.data_ptr()
+        med.c = float(np.max(m.values))
+        return med, coeffs
+
+    @staticmethod
+    def heterogeneous(domain: Domain) -> bool:
+        return domain.medium()[0] != "constant" or domain.lam != 0.0
+
+    def _chunks(self, domain: Domain, nt: int, nbeam: int, fp64: bool):
+        d = domain.ndim
+        S = d * (d + 1) // 2
+        n_tt = (nt + 31) // 32
+        per = nt * ((2 * d + 2 * d * d + 2) * 8 if fp64 else (16 * d + 8 * S + 8)) + n_tt * (2 * d + 1) * 4
+        chunk = max(1, min(nbeam, self.trajectory_memory // max(per, 1)))
+        return [(b, min(chunk, nbeam - b)) for b in range(0, nbeam, chunk)], per, n_tt
+
+    def _ode_opts(self, ts):
+        cfg = self.ode_config
+        if cfg.method == "rk4":
+            return _lib.OdeOpts(method=0, substeps=self.rk4_substeps)
+        return _lib.OdeOpts(method=1, substeps=1, rtol=float(cfg.rtol), atol=float(cfg.atol),
+                            dt0=float(cfg.dt0) if cfg.dt0 is not None else 0.0, max_steps=int(cfg.max_steps))
+
+    def _trajectories(self, pr, med, bs, b_first, nb, fp64, per, n_tt, dev, st, status):
+        buf = workspace(dev, "traj", per * nb + 4096)
+        base = buf.data_ptr()
+        d = pr.ndim
+        S = d * (d + 1) // 2
+        rec_bytes = pr.nt * nb * ((2 * d + 2 * d * d + 2) * 8 if fp64 else (16 * d + 8 * S + 8))
+        cull_off = (rec_bytes + 255) // 256 * 256
+        tr = _lib.Trajectories(nb=nb, b_first=b_first, rec64=base if fp64 else None, rec32=None if fp64 else base,
+                               cull=None if fp64 else base + cull_off,
+                               status=status.data_ptr() + 4 * b_first)
+        opts = self._ode_opts(None)
+        _lib.check(_lib.lib().msgb_ode_trajectories(_lib.ref(pr), _lib.ref(med), _lib.ref(bs), _lib.ref(opts),
+                                                    _lib.ref(tr), st), "msgb_ode_trajectories")
+        return tr, buf
+
+    def _check_status(self, status):
+        """Raise, as the reference's diffeqsolve does, when an integration failed."""
+        worst = int(status.max().item()) if status.numel() else 0
+        if worst == 2:
+            n = int((status == 2).sum().item())
+            raise RuntimeError(f"ODE integration reached max_steps={self.ode_config.max_steps} for {n} beam(s); "
+                               "raise SolverConfig.max_steps or loosen rtol/atol")
+        if worst == 1:
+            n = int((status == 1).sum().item())
+            raise RuntimeError(f"ODE integration produced a non-finite state for {n} beam(s); "
+                               "increase rk4_substeps or use an adaptive solver")
+
+    def _sum_forward_het(self, bt: BeamTensors, domain: Domain, sensors, ts):
+        import torch
+
+        dev = bt.x0.device
+        pr, keep = self._problem(domain, sensors, ts, dev)
+        med, keep_m = self._medium(domain, dev)
+        bs = bt.beam_set(unit=False)
+        st = torch.cuda.current_stream(dev).cuda_stream
+        fp64 = self.precision == "fp64"
+        chunks, per, n_tt = self._chunks(domain, pr.nt, 2 * bt.n, fp64)
+        status = torch.zeros(2 * bt.n, dtype=torch.int32, device=dev)
+        if fp64:
+            out = torch.zeros((pr.nt, pr.ns), dtype=torch.float64, device=dev)
+            for b_first, nb in chunks:
+                tr, _ = self._trajectories(pr, med, bs, b_first, nb, True, per, n_tt, dev, st, status)
+                _lib.check(_lib.lib().msgb_sum_fwd_f64_traj(_lib.ref(pr), _lib.ref(bs), _lib.ref(tr), out.data_ptr(),
+                                                            st), "msgb_sum_fwd_f64_traj")
+            self._check_status(status)
+            return out
+        out = torch.empty((pr.nt, pr.ns), dtype=torch.float32, device=dev)
+        cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+        tiling = self._tiling(domain, sensors, dev)
+        opts = _lib.SumOpts(cutoff=self.cutoff, eval_count=cnt.data_ptr(),
+                            tiling=_lib.ref(tiling[0]) if tiling else None)
+        nbytes = _lib.lib().msgb_sum_f32_traj_workspace_size(_lib.ref(pr), 2 * bt.n)
+        ws = workspace(dev, "sum32traj", nbytes)
+        for i, (b_first, nb) in enumerate(chunks):
+            tr, _ = self._trajectories(pr, med, bs, b_first, nb, False, per, n_tt, dev, st, status)
+            _lib.check(_lib.lib().msgb_sum_fwd_f32_traj(_lib.ref(pr), _lib.ref(bs), _lib.ref(tr), _lib.ref(opts),
+                                                        int(i == 0), int(i == len(chunks) - 1), ws.data_ptr(), nbytes,
+                                                        out.data_ptr(), st), "msgb_sum_fwd_f32_traj")
+        self._eval_counter = cnt
+        self._check_status(status)
+        return out
+
+    def _gather_adjoint_het(self, bt: BeamTensors, domain: Domain, sensors, ts, data):
+        import torch
+
+        dev = bt.x0.device
+        pr, keep = self._problem(domain, sensors, ts, dev)
+        med, keep_m = self._medium(domain, dev)
+        bs = bt.beam_set(unit=True)
+        st = torch.cuda.current_stream(dev).cuda_stream
+        fp64 = self.precision == "fp64"
+        n = bt.n
+        chunks, per, n_tt = self._chunks(domain, pr.nt, 2 * n, fp64)
+        g_all = torch.empty(2 * n, dtype=torch.complex128, device=dev)
+        if fp64:
+            d = as_device_f64(data, dev).reshape(pr.nt, pr.ns).contiguous()
+        elif isinstance(data, torch.Tensor) and data.is_cuda and data.dtype == torch.float32:
+            d = data.reshape(pr.nt, pr.ns).contiguous()
+        else:
+            d = as_device_f64(data, dev).to(torch.float32).reshape(pr.nt, pr.ns).contiguous()
+        cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+        tiling = None if fp64 else self._tiling(domain, sensors, dev)
+        opts = _lib.SumOpts(cutoff=self.cutoff, eval_count=cnt.data_ptr(),
+                            tiling=_lib.ref(tiling[0]) if tiling else None)
+        nbytes = 0 if fp64 else _lib.lib().msgb_sum_f32_traj_workspace_size(_lib.ref(pr), 2 * n)
+        ws = None if fp64 else workspace(dev, "sum32traj", nbytes)
+        status = torch.zeros(2 * n, dtype=torch.int32, device=dev)
+        for b_first, nb in chunks:
+            tr, _ = self._trajectories(pr, med, bs, b_first, nb, fp64, per, n_tt, dev, st, status)
+            gp = torch.view_as_real(g_all[b_first:b_first + nb]).data_ptr()
+            if fp64:
+                _lib.check(_lib.lib().msgb_adj_gather_f64_traj(_lib.ref(pr), _lib.ref(bs), _lib.ref(tr), d.data_ptr(),
+                                                               gp, st), "msgb_adj_gather_f64_traj")
+            else:
+                _lib.check(_lib.lib().msgb_adj_gather_f32_traj(_lib.ref(pr), _lib.ref(bs), _lib.ref(tr), _lib.ref(opts),
+                                                               ws.data_ptr(), nbytes, d.data_ptr(), gp, st),
+                           "msgb_adj_gather_f32_traj")
+        self._eval_counter = cnt
+        self._check_status(status)
+        return g_all[:n] + g_all[n:]
+
     def sum_forward(self, bt: BeamTensors, domain: Domain, sensors, ts):
         """Beam summation at the sensors: (Nt, Ns) float64 (fp64) or float32 (fp32)."""
         import torch
+
+        if self.heterogeneous(domain):
+            return self._sum_forward_het(bt, domain, sensors, ts)
 
         dev = bt.x0.device
         pr, keep = self._problem(domain, sensors, ts, dev)
@@ -302,6 +462,9 @@ class MSGBSolver:
     def gather_adjoint(self, bt: BeamTensors, domain: Domain, sensors, ts, data):
         """Per selected coefficient g_j = sum 2 d conj(K_j) over both modes: (n,) complex128."""
         import torch
+
+        if self.heterogeneous(domain):
+            return self._gather_adjoint_het(bt, domain, sensors, ts, data)
 
         dev = bt.x0.device
         pr, keep = self._problem(domain, sensors, ts, dev)

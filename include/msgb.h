@@ -121,7 +121,7 @@ int msgb_adj_gather_f32(const msgb_problem *prob, const msgb_beam_set *beams,
                         const msgb_sum_opts *opts, void *workspace, size_t workspace_bytes,
                         const float *data, double *g, msgb_stream_t stream);
 
-/* ---- heterogeneous media: RK4 beam propagation ------------------------- */
+/* ---- heterogeneous media: FP64 beam propagation ------------------------ */
 
 #define MSGB_TIME_TILE 32          /* time samples per culling record */
 
@@ -156,7 +156,8 @@ typedef struct msgb_medium {
  *          arg A and 2|A| (floats).
  *   cull:  (ceil(nt / MSGB_TIME_TILE), nb, 2d + 1) floats: bounding box of
  *          the centre over each time tile (lo, hi) and (w/2) min lambda_min(Im M).
- *   status: (nb) 0 ok, 1 non-finite state encountered. */
+ *   status: (nb) 0 ok, 1 non-finite state encountered, 2 max_steps reached
+ *          (the adaptive integrator; the state then stays at its last value). */
 typedef struct msgb_trajectories {
     int64_t nb;
     int64_t b_first;
@@ -166,8 +167,29 @@ typedef struct msgb_trajectories {
     int32_t *status;
 } msgb_trajectories;
 
-/* Fixed-step FP64 RK4 of coupled_rhs_absorption (gb/gb_solvers.py:787-867)
- * with step (ts[1] - ts[0]) / substeps, state recorded at every ts. */
+enum {
+    MSGB_ODE_RK4 = 0,              /* fixed step: `substeps` equal steps per save interval */
+    MSGB_ODE_DOPRI5 = 1            /* adaptive Dormand-Prince 5(4) */
+};
+
+/* Integrator settings; the adaptive fields mirror SolverConfig
+ * (gb/gb_solvers.py:597-632: rtol 1e-7, atol 1e-9, max_steps 4096, dt0). */
+typedef struct msgb_ode_opts {
+    int32_t method;
+    int32_t substeps;        /* RK4 */
+    double rtol, atol;       /* DOPRI5: error norm RMS |e| / (atol + rtol max(|y0|, |y1|)) */
+    double dt0;              /* DOPRI5 first step; <= 0 selects ts[1] - ts[0] */
+    int64_t max_steps;       /* DOPRI5: accepted + rejected steps per beam */
+} msgb_ode_opts;
+
+/* FP64 integration of coupled_rhs_absorption (gb/gb_solvers.py:787-867) for
+ * each beam, state recorded at every ts; replaces solve_ODE_base
+ * (gb/gb_solvers.py:940-1014, diffrax Tsit5 with PIDController and
+ * SaveAt(ts)).  One thread per beam. */
+int msgb_ode_trajectories(const msgb_problem *prob, const msgb_medium *med, const msgb_beam_set *beams,
+                          const msgb_ode_opts *opts, const msgb_trajectories *out, msgb_stream_t stream);
+
+/* msgb_ode_trajectories with method MSGB_ODE_RK4 and the given substeps. */
 int msgb_rk4_trajectories(const msgb_problem *prob, const msgb_medium *med, const msgb_beam_set *beams,
                           int substeps, const msgb_trajectories *out, msgb_stream_t stream);
 
@@ -195,6 +217,38 @@ int msgb_adj_gather_f32_traj(const msgb_problem *prob, const msgb_beam_set *beam
                              const msgb_trajectories *traj, const msgb_sum_opts *opts,
                              void *workspace, size_t workspace_bytes, const float *data, double *g,
                              msgb_stream_t stream);
+
+/* ---- tensor-core BF16 GEMM and MLP kernels (trajectory surrogate) ------ */
+
+/* C = A B^T (+ bias) on the tcgen05 tensor cores, FP32 accumulation in tensor
+ * memory.  A (M x K) and B (N x K) are BF16 with element strides (sAm, sAk)
+ * and (sBn, sBk); N is a multiple of 16 in [16, 256].  C32 receives the FP32
+ * pre-activation, C16 the BF16 activation (act 0: identity, 1: SiLU). */
+typedef struct msgb_gemm {
+    const void *A;
+    int64_t sAm, sAk;
+    const void *B;
+    int64_t sBn, sBk;
+    int32_t M, N, K;
+    const float *bias;
+    int32_t act;
+    float *C32;
+    int64_t ldc32;
+    void *C16;
+    int64_t ldc16;
+    int *error_flag;  /* device int, set to 1 if a tensor-core wait ran out; may be NULL */
+} msgb_gemm;
+
+int msgb_gemm_bf16(const msgb_gemm *p, msgb_stream_t stream);
+/* dZ = dA * silu'(Z) elementwise (FP32 in; FP32 and/or BF16 out). */
+int msgb_silu_backward(const float *dA, const float *Z, int64_t n, float *dZ32, void *dZ16,
+                       msgb_stream_t stream);
+/* out[n] = sum_m X[m, n], fixed order. */
+int msgb_colsum(const float *X, int M, int N, int64_t ld, float *out, msgb_stream_t stream);
+/* Adam step (FP32 master weights, optional BF16 copy). */
+int msgb_adam(float *w, const float *g, float *m1, float *m2, int64_t n, double lr, double b1, double b2,
+              double eps, int64_t step, void *w16, msgb_stream_t stream);
+int msgb_to_bf16(const float *x, int64_t n, void *y, msgb_stream_t stream);
 
 /* ---- MSWPT tiling (transforms.py:357-850) ------------------------------ */
 

@@ -178,3 +178,129 @@ def beam_field(xt, pt, Mt, At, omega, sensors, domain_size, periodic):
 
     return gaussian_beam_real_sum(xt[None], pt[None], Mt[None], At[None, :, None], np.array([omega]),
                                   np.asarray(sensors), domain_size, periodic)
+
+
+def _unpack_states(Y, d):
+    Y = np.asarray(Y)
+    xt = Y[:, :d]
+    pt = Y[:, d:2 * d]
+    Mt = (Y[:, 2 * d:2 * d + d * d] + 1j * Y[:, 2 * d + d * d:2 * d + 2 * d * d]).reshape(-1, d, d)
+    At = Y[:, -2] + 1j * Y[:, -1]
+    return xt, pt, Mt, At
+
+
+def _pack_state(x0, p0, M0, a0):
+    M0 = np.asarray(M0, complex)
+    return np.concatenate([x0, p0, M0.real.ravel(), M0.imag.ravel(), [np.real(a0), np.imag(a0)]]).astype(float)
+
+
+def rk4(x0, p0, M0, a0, mode, ts, speed, substeps=1, lam=0.0):
+    """Fixed-step RK4 of ``rhs``, ``substeps`` equal steps per interval [ts[k-1], ts[k]].
+
+    The same method as the GPU integrator's fixed-step option; used to separate
+    the method's own error (a cubic B-spline medium is only C^2, so RK4 loses
+    order where hess c has kinks) from implementation differences.
+    """
+    d = len(x0)
+    y = _pack_state(x0, p0, M0, a0)
+    ts = np.asarray(ts, float)
+    f = lambda v: rhs(0.0, v, mode, speed, d, lam)
+    out = [y.copy()]
+    for k in range(1, ts.size):
+        h = (ts[k] - ts[k - 1]) / substeps
+        for _ in range(substeps):
+            k1 = f(y)
+            k2 = f(y + 0.5 * h * k1)
+            k3 = f(y + 0.5 * h * k2)
+            k4 = f(y + h * k3)
+            y = y + h / 6.0 * (k1 + 2 * k2 + 2 * k3 + k4)
+        out.append(y.copy())
+    return _unpack_states(out, d)
+
+
+# Dormand & Prince (1980) 5(4) pair: nodes, stage matrix, 5th-order weights
+# (= the last stage row, first-same-as-last) and the 4th-order embedded weights.
+DP_C = (0.0, 1 / 5, 3 / 10, 4 / 5, 8 / 9, 1.0, 1.0)
+DP_A = ((),
+        (1 / 5,),
+        (3 / 40, 9 / 40),
+        (44 / 45, -56 / 15, 32 / 9),
+        (19372 / 6561, -25360 / 2187, 64448 / 6561, -212 / 729),
+        (9017 / 3168, -355 / 33, 46732 / 5247, 49 / 176, -5103 / 18656),
+        (35 / 384, 0.0, 500 / 1113, 125 / 192, -2187 / 6784, 11 / 84))
+DP_B = (35 / 384, 0.0, 500 / 1113, 125 / 192, -2187 / 6784, 11 / 84, 0.0)
+DP_BHAT = (5179 / 57600, 0.0, 7571 / 16695, 393 / 640, -92097 / 339200, 187 / 2100, 1 / 40)
+DP_E = tuple(b - bh for b, bh in zip(DP_B, DP_BHAT))
+
+
+def error_norm(e, y0, y1, d, rtol, atol):
+    """RMS over the complex state entries (x, p, M, A) of |e| / (atol + rtol max(|y0|, |y1|)),
+    the norm diffrax's PIDController applies (optimistix.rms_norm)."""
+    def mags(v):
+        x = np.abs(v[:2 * d])
+        M = np.hypot(v[2 * d:2 * d + d * d], v[2 * d + d * d:2 * d + 2 * d * d])
+        A = np.hypot(v[-2], v[-1])
+        return np.concatenate([x, M, [A]])
+    r = mags(e) / (atol + rtol * np.maximum(mags(y0), mags(y1)))
+    return float(np.sqrt(np.mean(r * r)))
+
+
+def dopri5(x0, p0, M0, a0, mode, ts, speed, lam=0.0, rtol=1e-7, atol=1e-9, max_steps=4096, dt0=None):
+    """Adaptive Dormand-Prince 5(4) of ``rhs`` with the state saved at every ts.
+
+    Step control (the GPU integrator's, step for step): error norm as
+    ``error_norm``; accept when it is <= 1; next step h * clip(0.9 err^(-1/5),
+    0.2, 10) (at most 1 after a rejection); steps are shortened to land on each
+    save time, and after such a landing the previous proposal is kept if larger.
+    ``max_steps`` counts accepted and rejected steps over the whole solve, as
+    diffrax does (gb/gb_solvers.py:756-783 builds that solve: Tsit5,
+    PIDController(rtol, atol), SaveAt(ts), dt0 = ts[1] - ts[0]).
+    Returns (xt, pt, Mt, At, status, steps); status 0 ok, 1 non-finite,
+    2 max_steps reached.
+    """
+    d = len(x0)
+    y = _pack_state(x0, p0, M0, a0)
+    ts = np.asarray(ts, float)
+    f = lambda v: rhs(0.0, v, mode, speed, d, lam)
+    h = float(dt0) if dt0 is not None else (ts[1] - ts[0] if ts.size > 1 else 0.0)
+    out = [y.copy()]
+    steps, status = 0, 0
+    k1 = f(y)
+    t = ts[0]
+    for k in range(1, ts.size):
+        t_end = ts[k]
+        while status == 0 and t < t_end:
+            if steps >= max_steps:
+                status = 2
+                break
+            hh, clipped = h, False
+            if t + hh >= t_end:
+                hh, clipped = t_end - t, True
+            ks = [k1]
+            for s in range(1, 7):
+                acc = np.zeros_like(y)
+                for j, a in enumerate(DP_A[s]):
+                    if a != 0.0:
+                        acc = acc + a * ks[j]
+                ks.append(f(y + hh * acc))
+            y5 = y + hh * sum(b * kk for b, kk in zip(DP_B, ks) if b != 0.0)
+            # stage 7 is evaluated at y + hh * sum(a7j k_j), which is y5 up to rounding
+            e = hh * sum(c * kk for c, kk in zip(DP_E, ks))
+            err = error_norm(e, y, y5, d, rtol, atol)
+            steps += 1
+            if not np.isfinite(err):
+                h = 0.2 * hh
+                continue
+            fac = 10.0 if err == 0.0 else min(10.0, max(0.2, 0.9 * err ** -0.2))
+            if err <= 1.0:
+                t = t_end if clipped else t + hh
+                y = y5
+                k1 = ks[6]
+                hn = hh * fac
+                h = max(hn, h) if clipped else hn
+            else:
+                h = hh * min(1.0, fac)
+        if status == 0 and not np.all(np.isfinite(y)):
+            status = 1
+        out.append(y.copy())
+    return _unpack_states(out, d) + (status, steps)

@@ -141,3 +141,30 @@ def test_adjoint_reference_signature_is_explicitly_not_this_operator():
     s = bb.MSGBSolver(4, "top_n", 4, "spatial", "solve_hom_diag", "all_real")
     with pytest.raises(NotImplementedError, match="principal-symbol"):
         s.adjoint(np.zeros((3, 1)), d, np.zeros((1, 1)), object(), np.arange(3.0), d, w)
+
+
+def test_solver_config_matches_reference_checks():
+    """SolverConfig (gb/gb_solvers.py:597-703): defaults, validation, precision presets."""
+    from beamax_b200.gb.gb_solvers import SolverConfig, ode_method
+
+    cfg = SolverConfig()
+    assert (cfg.rtol, cfg.atol, cfg.max_steps, cfg.dt0) == (1e-7, 1e-9, 4096, None)
+    assert cfg.method == "dopri5"
+    assert SolverConfig.from_precision(use_x64=False).rtol == 1e-4
+    assert SolverConfig.from_precision(rtol=1e-5, max_steps=10000).max_steps == 10000
+    assert SolverConfig(solver="rk4", substeps=4).method == "rk4"
+    for bad in ({"max_steps": 0}, {"max_steps": True}, {"rtol": 0.0}, {"atol": float("nan")}, {"dt0": -1.0},
+                {"pcoeff": float("inf")}, {"solver": "euler"}, {"substeps": 0}):
+        with pytest.raises(ValueError):
+            SolverConfig(**bad)
+    with pytest.raises(NotImplementedError):
+        SolverConfig(pcoeff=0.3)
+
+    class Tsit5:
+        pass
+
+    assert ode_method(Tsit5()) == "dopri5"
+    solver = bb.MSGBSolver(8, "top_n", 8, "spatial", bb.gb.gb_solvers.solve_ODE_base, "scan_real")
+    assert solver.ode_config == SolverConfig()
+    with pytest.raises(TypeError):
+        bb.MSGBSolver(8, "top_n", 8, "spatial", bb.gb.gb_solvers.solve_ODE_base, "scan_real", ode_config={})

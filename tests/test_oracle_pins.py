@@ -248,3 +248,46 @@ def test_adjoint_dot_product_2d():
     lhs = np.sum(om.forward_hom(om.beams_for(bm.idx, om.compute_coefficients(q, np.zeros(N), "spatial", dom, w, "pos_only")[bm.idx], dom, w), dom, sens, ts) * d)
     rhs = np.sum(q * om.adjoint(bm, dom, sens, ts, w, d))
     assert abs(lhs - rhs) <= 1e-12 * max(abs(lhs), abs(rhs))
+
+
+def test_oracle_dopri5_1d_linear_closed_form():
+    """Adaptive Dormand-Prince 5(4) against the closed form for c = a + b x
+    (tests/test_gb.py:630-756)."""
+    from oracle import ode as oo
+
+    a, b = 1.0, 1.0
+    xs = np.arange(0, 400) * 0.01
+    speed = oo.GridSpeed(a + b * xs, (0.01,), method="linear", boundary="clamp")
+    ts = np.linspace(0.0, 1.0, 200)
+    x, p, M, A, status, steps = oo.dopri5(np.array([0.1]), np.array([1.2]), np.array([[0.2j]]), 1.0, 1.0, ts, speed)
+    xr, pr, Mr, Ar = oo.analytic_1d_linear(0.1, 1.2, 0.2j, 1.0, ts, a, b)
+    assert status == 0 and steps >= ts.size - 1
+    assert np.allclose(x[:, 0], xr, atol=1e-10, rtol=1e-7)
+    assert np.allclose(p[:, 0], pr, atol=1e-10, rtol=1e-7)
+    assert np.allclose(M[:, 0, 0], Mr, atol=1e-10, rtol=1e-7)
+    assert np.allclose(A, Ar, atol=1e-10, rtol=1e-7)
+
+
+def test_oracle_dopri5_converges_to_dop853_and_honours_max_steps():
+    """Tighter tolerances move the adaptive solution onto DOP853's; a step
+    budget that is too small reports status 2."""
+    from scipy import ndimage
+
+    from oracle import ode as oo
+
+    rng = np.random.default_rng(5)
+    g = ndimage.gaussian_filter(rng.standard_normal((32, 32)), 8.0, mode="wrap")
+    c = 1500.0 * (1 + 0.1 * g / np.max(np.abs(g)))
+    speed = oo.GridSpeed(c, (1e-4, 1e-4), method="bspline3", boundary="clamp")
+    x0, p0, M0 = np.array([16e-4, 15e-4]), np.array([2 * np.pi, 0.3]), np.diag([1e-3j, 2e-3j])
+    ts = np.arange(0, 30) * 2e-8
+    xt, pt, Mt, At = oo.solve(x0, p0, M0, 1.0, 1.0, ts, speed)
+    errs = []
+    for rtol in (1e-6, 1e-9):
+        x, p, M, A, status, _ = oo.dopri5(x0, p0, M0, 1.0, 1.0, ts, speed, rtol=rtol, atol=rtol * 1e-2,
+                                          max_steps=100000)
+        assert status == 0
+        errs.append(np.max(np.abs(M - Mt)) / np.max(np.abs(Mt)))
+    assert errs[1] < 0.1 * errs[0]
+    *_, status, steps = oo.dopri5(x0, p0, M0, 1.0, 1.0, ts, speed, max_steps=5)
+    assert status == 2 and steps == 5
