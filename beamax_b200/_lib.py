@@ -87,6 +87,7 @@ SIGNATURES = {
     "msgb_sum_f32_workspace_size": (c_sz, [c_vp, c_i64]),
     "msgb_sum_fwd_f32": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_sz, c_vp, c_vp]),
     "msgb_adj_gather_f32": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_sz, c_vp, c_vp, c_vp]),
+    "msgb_sum_fwd_f32_static": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp]),
     "msgb_rk4_trajectories": (ctypes.c_int, [c_vp, c_vp, c_vp, ctypes.c_int, c_vp, c_vp]),
     "msgb_ode_trajectories": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "msgb_sum_fwd_f64_traj": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp]),

@@ -28,6 +28,8 @@
 // skipped when that bound exceeds `cutoff` e-folds.
 #include <cub/cub.cuh>
 
+#include <mutex>
+
 #include "common.cuh"
 
 namespace msgb {
@@ -1148,3 +1150,69 @@ extern "C" int msgb_adj_gather_f32_traj(const msgb_problem *prob, const msgb_bea
     }
 }
 
+// ---- forward summation for callers that cannot allocate ----------------------
+//
+// Some hosts cannot hand this library device memory: an XLA custom-call or
+// plugin handler registered without a scratch allocator, a runtime whose
+// device memory belongs entirely to another framework's pool, or a process
+// with allocation forbidden once serving starts.  For them the FP32 forward
+// takes its scratch from the fixed array below instead of a caller workspace.
+// The array is part of the module: every GPU that loads the library holds it
+// until the process exits.  In host code `sum32_static_scratch` only stands in
+// for the symbol; the device address comes from cudaGetSymbolAddress, taken
+// once per device on the first call made with that device current.
+static __device__ __align__(256) unsigned char sum32_static_scratch[MSGB_SUM_F32_STATIC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kMaxStaticDevices = 64;
+std::mutex static_scratch_mu;
+void *static_scratch_ptr[kMaxStaticDevices] = {};
+
+int static_scratch_address(void **ptr) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(MSGB_ERR_CUDA, "msgb_sum_fwd_f32_static: cudaGetDevice: %s", cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxStaticDevices)
+        return fail(MSGB_ERR_UNSUPPORTED, "msgb_sum_fwd_f32_static: device ordinal %d beyond %d", dev,
+                    kMaxStaticDevices - 1);
+    std::lock_guard<std::mutex> lock(static_scratch_mu);
+    if (!static_scratch_ptr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, sum32_static_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(MSGB_ERR_CUDA, "msgb_sum_fwd_f32_static: cudaGetSymbolAddress on device %d: %s", dev,
+                        cudaGetErrorString(e));
+        static_scratch_ptr[dev] = p;
+    }
+    *ptr = static_scratch_ptr[dev];
+    return MSGB_OK;
+}
+}  // namespace
+
+extern "C" int msgb_sum_fwd_f32_static(const msgb_problem *prob, const msgb_beam_set *beams,
+                                       const msgb_sum_opts *opts, float *out, msgb_stream_t stream) {
+    if (int e = validate_problem(prob)) return e;
+    if (int e = validate_beams(prob, beams)) return e;
+    if (!out) return fail(MSGB_ERR_ARG, "msgb_sum_fwd_f32_static: out is NULL");
+    if (prob->nt == 0 || prob->ns == 0) return MSGB_OK;
+    const Layout need = layout(prob, beams->n, false, tile_count(prob, opts));
+    if (need.total > (size_t)MSGB_SUM_F32_STATIC_SCRATCH_BYTES)
+        return fail(MSGB_ERR_UNSUPPORTED,
+                    "msgb_sum_fwd_f32_static: %lld coefficients and %lld sensors need %zu bytes of scratch, more "
+                    "than the %zu-byte static scratch; call msgb_sum_fwd_f32 with a workspace instead",
+                    (long long)beams->n, (long long)prob->ns, need.total, (size_t)MSGB_SUM_F32_STATIC_SCRATCH_BYTES);
+    void *scratch = nullptr;
+    if (int e = static_scratch_address(&scratch)) return e;
+    Layout l;
+    if (int e = check_ws(prob, beams, opts, false, scratch, MSGB_SUM_F32_STATIC_SCRATCH_BYTES, l)) return e;
+    // Only the persistent kernel's work counter must start at zero; run_fwd
+    // clears it on the stream before the launch.  Everything else in the
+    // scratch is written by this call's preparation kernels before it is read.
+    cudaStream_t st = as_stream(stream);
+    char *ws = (char *)scratch;
+    switch (prob->ndim) {
+        case 1: return run_fwd<1, false>(prob, beams, opts, ws, l, out, st, traj_src<1>(nullptr, nullptr, 1, 1));
+        case 2: return run_fwd<2, false>(prob, beams, opts, ws, l, out, st, traj_src<2>(nullptr, nullptr, 1, 1));
+        default: return run_fwd<3, false>(prob, beams, opts, ws, l, out, st, traj_src<3>(nullptr, nullptr, 1, 1));
+    }
+}

@@ -115,6 +115,31 @@ int msgb_sum_fwd_f32(const msgb_problem *prob, const msgb_beam_set *beams,
                      const msgb_sum_opts *opts, void *workspace, size_t workspace_bytes,
                      float *out, msgb_stream_t stream);
 
+/* msgb_sum_fwd_f32 for callers that cannot allocate device memory: no
+ * counterpart in the reference.  Meant for hosts that have no allocator to
+ * give this library (an XLA custom call registered without a scratch buffer,
+ * a runtime whose device memory is owned by another framework's pool, a
+ * server that forbids allocation after start-up).  It calls no cudaMalloc,
+ * cudaFree or allocating library routine; its scratch is a fixed array of
+ * MSGB_SUM_F32_STATIC_SCRATCH_BYTES inside the library, resident on every GPU
+ * that loads the library until the process exits.  Same inputs, output and
+ * numerics as msgb_sum_fwd_f32 on the current device.
+ *   - Limit: problems whose forward scratch exceeds the array are rejected
+ *     with MSGB_ERR_UNSUPPORTED and a message giving the bytes needed (about
+ *     44 B per coefficient plus 50-70 B per sensor: 65536 coefficients and
+ *     2044 sensors take about 3 MB, and 16 MiB holds about 370000
+ *     coefficients at that sensor count).
+ *   - The first call on each device, with that device current, looks up the
+ *     array's device address (cudaGetSymbolAddress); make that first call
+ *     before any stream capture.
+ *   - Every call shares the one array, which keeps the last call's contents
+ *     (the call clears what must start at zero).  Calls whose executions
+ *     overlap on the GPU (different streams, or concurrent host threads)
+ *     race on it: order them on one stream or with events. */
+#define MSGB_SUM_F32_STATIC_SCRATCH_BYTES (16u << 20)
+int msgb_sum_fwd_f32_static(const msgb_problem *prob, const msgb_beam_set *beams,
+                            const msgb_sum_opts *opts, float *out, msgb_stream_t stream);
+
 /* FP32 transpose of msgb_sum_fwd_f32 (same culling); one owner per beam, no
  * atomics.  data: (nt, ns) FP32.  g: (n) complex FP64. */
 int msgb_adj_gather_f32(const msgb_problem *prob, const msgb_beam_set *beams,
