@@ -267,13 +267,21 @@ __device__ __forceinline__ void anchor(const ProbArgs &P, const BeamTime<D> &bt,
 // sensor spacing over a 16-sensor run, e.g. after focusing in a
 // heterogeneous medium) reach it.
 constexpr float kRecurrenceEfolds = 60.0f;
+// A run whose smallest exponent over its 16 sensors exceeds this many e-folds
+// contributes below 4e-18 of the beam's amplitude and is skipped (only when
+// culling is enabled, cutoff > 0).
+constexpr float kNegligibleEfolds = 40.0f;
+
+enum RunKind { kRunRecurrence = 0, kRunNegligible = 1, kRunDirect = 2 };
 
 // Direct evaluation at a run start (seed): z, and the recurrence factors for
-// the step h to the next sensor.  With `safe`, reports whether the recurrence
-// stays within kRecurrenceEfolds.
+// the step h to the next sensor.  With `kind`, classifies the run of GS
+// sensors (RunKind): the exponent along it is chi(k) = chi + B k + A k^2 with
+// B = -a1r, A = -a2r.
 template <int D, bool PERIODIC>
 __device__ __forceinline__ cf seed_eval(const Rec<D> &r, const float *ds, const float *h, bool cont,
-                                        const ProbArgs &P, cf &rr, cf &qq, bool *safe = nullptr) {
+                                        const ProbArgs &P, cf &rr, cf &qq, int *kind = nullptr,
+                                        bool skip_negligible = false) {
     float Dl[D];
     float th = r.th0;
 #pragma unroll
@@ -295,8 +303,18 @@ __device__ __forceinline__ cf seed_eval(const Rec<D> &r, const float *ds, const 
         const float a2r = -quad<D>(r.p, h), a2i = quad<D>(r.q, h);
         rr = cexpf_(a1r + a2r, a1i + a2i);
         qq = cexpf_(2.0f * a2r, 2.0f * a2i);
-        if (safe)
-            *safe = chi <= kRecurrenceEfolds && a1r + a2r <= kRecurrenceEfolds && -2.0f * a2r <= kRecurrenceEfolds;
+        if (kind) {
+            const float Aq = -a2r, Bq = -a1r;
+            const float kv = Aq > 0.0f ? fminf(fmaxf(-Bq / (2.0f * Aq), 0.0f), (float)(GS - 1)) : 0.0f;
+            const float kl = (float)(GS - 1);
+            const float chi_min = fminf(fminf(chi, chi + kl * (Bq + Aq * kl)), chi + kv * (Bq + Aq * kv));
+            if (skip_negligible && chi_min > kNegligibleEfolds)
+                *kind = kRunNegligible;
+            else if (chi > kRecurrenceEfolds || a1r + a2r > kRecurrenceEfolds || -2.0f * a2r > kRecurrenceEfolds)
+                *kind = kRunDirect;
+            else
+                *kind = kRunRecurrence;
+        }
     }
     return z;
 }
@@ -638,12 +656,14 @@ fwd32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
                         load_rec<D>(rec, gl, lane, ra);
                         load_rec<D>(rec, gl + 1, lane, rb);  // zero-amplitude record when gl + 1 == ng
                         cf za, fa, qa, zb, fb, qb;
-                        bool oka = true, okb = true;
+                        int ka = kRunRecurrence, kb = kRunRecurrence;
                         if (fast) {
-                            za = seed_eval<D, false>(ra, sds[gbase], shn[gbase], true, P, fa, qa, &oka);
-                            zb = seed_eval<D, false>(rb, sds[gbase], shn[gbase], true, P, fb, qb, &okb);
+                            za = seed_eval<D, false>(ra, sds[gbase], shn[gbase], true, P, fa, qa, &ka, cutoff > 0.0f);
+                            zb = seed_eval<D, false>(rb, sds[gbase], shn[gbase], true, P, fb, qb, &kb, cutoff > 0.0f);
+                            if (ka == kRunNegligible) za = fa = qa = cf{0.0f, 0.0f};
+                            if (kb == kRunNegligible) zb = fb = qb = cf{0.0f, 0.0f};
                         }
-                        if (fast && oka && okb) {
+                        if (fast && ka != kRunDirect && kb != kRunDirect) {
                             kahan_add(acc[0], cmp[0], za.re + zb.re);
 #pragma unroll
                             for (int k = 1; k < GS; ++k) {
@@ -701,15 +721,22 @@ template <int D, bool PERIODIC, bool TRAJ>
 __global__ void __launch_bounds__(THREADS)
 adj32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *tiles, const int32_t *offs,
              int64_t n_st, const float *ds_g, const float *hn_g, const uint8_t *gfast_g, const float *dataT,
-             float cutoff, double *g, unsigned long long *eval_count, TrajSrc<D> T) {
+             float cutoff, double *g, unsigned long long *eval_count, unsigned long long *work, TrajSrc<D> T) {
     constexpr int CH = 4;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t j = (int64_t)blockIdx.x * NW + warp;
-    if (j >= (TRAJ ? T.nb : B.n)) return;
+    const int lane = threadIdx.x & 31;
+    const int64_t n_owned = TRAJ ? T.nb : B.n;
+    unsigned long long evals = 0;
+    // Persistent warps: each takes the next beam from a global counter, so
+    // the uneven per-beam work (coarse beams cross many more tiles) does not
+    // leave warps idle at the end of a statically assigned block.
+    for (;;) {
+    unsigned long long jj = 0;
+    if (lane == 0) jj = atomicAdd(work, 1ull);
+    const int64_t j = (int64_t)__shfl_sync(0xffffffffu, jj, 0);
+    if (j >= n_owned) break;
     const Cull<D> cb = TRAJ ? Cull<D>{} : cull[j];
     const int64_t n_tt = (P.nt + TT - 1) / TT;
     double gre = 0.0, gim = 0.0;
-    unsigned long long evals = 0;
     for (int m = 0; m < (TRAJ ? 1 : 2); ++m) {
         const float c0 = m == 0 ? (float)P.c : -(float)P.c;
         const int64_t b = m == 0 ? j : j + B.n;
@@ -763,9 +790,10 @@ adj32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
 #pragma unroll
                                 for (int i = 0; i < D; ++i)
                                     dsl[i] = __ldg(ds_g + (s_first + s) * D + i), hl[i] = __ldg(hn_g + (s_first + s) * D + i);
-                                bool okc = true;
-                                z[c] = seed_eval<D, false>(r, dsl, hl, true, P, rr[c], qq[c], &okc);
-                                ok = ok && okc;
+                                int kc = kRunRecurrence;
+                                z[c] = seed_eval<D, false>(r, dsl, hl, true, P, rr[c], qq[c], &kc, cutoff > 0.0f);
+                                if (kc == kRunNegligible) z[c] = rr[c] = qq[c] = cf{0.0f, 0.0f};
+                                ok = ok && kc != kRunDirect;
                                 d[c] = tv ? __ldg(dcol + (int64_t)s * P.nt) : 0.0f;
                             }
                             if (!ok) {
@@ -826,13 +854,15 @@ adj32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
     for (int o = 16; o > 0; o >>= 1) {
         gre += __shfl_down_sync(0xffffffffu, gre, o);
         gim += __shfl_down_sync(0xffffffffu, gim, o);
-        evals += __shfl_down_sync(0xffffffffu, evals, o);
     }
     if (lane == 0) {
         g[2 * j] = gre;
         g[2 * j + 1] = gim;
-        if (eval_count && evals) atomicAdd(eval_count, evals);
     }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) evals += __shfl_down_sync(0xffffffffu, evals, o);
+    if (lane == 0 && eval_count && evals) atomicAdd(eval_count, evals);
 }
 
 // ------------------------------------------------------------------ workspace
@@ -990,13 +1020,17 @@ int run_adj(const msgb_problem *p, const msgb_beam_set *b, const msgb_sum_opts *
     bool periodic = false;
     for (int i = 0; i < D; ++i) periodic |= (p->periodic[i] != 0);
     const int64_t nw = TRAJ ? T.nb : b->n;
-    const unsigned grid = (unsigned)((nw + NW - 1) / NW);
+    unsigned long long *work = (unsigned long long *)(ws + l.work + 8);
+    cudaMemsetAsync(work, 0, sizeof(unsigned long long), st);
+    const int64_t want = 2LL * sm_count();
+    const int64_t need = (nw + NW - 1) / NW;
+    const unsigned grid = (unsigned)(need < want ? need : want);
     auto args = [&](auto kern) {
         kern<<<grid, THREADS, 0, st>>>(P, to_args(b), (const Cull<D> *)(ws + l.cull), (const TileInfo<D> *)(ws + l.tiles),
                                        (const int32_t *)(ws + l.offs), l.n_st, (const float *)(ws + l.ds),
                                        (const float *)(ws + l.hn), (const uint8_t *)(ws + l.gfast),
                                        (const float *)(ws + l.data), o ? (float)o->cutoff : 0.0f, g,
-                                       o ? o->eval_count : nullptr, T);
+                                       o ? o->eval_count : nullptr, work, T);
     };
     if (periodic)
         args(adj32_kernel<D, true, TRAJ>);
