@@ -59,7 +59,15 @@ class Medium(ctypes.Structure):
 
 class OdeOpts(ctypes.Structure):
     _fields_ = [("method", c_i32), ("substeps", c_i32), ("rtol", c_dbl), ("atol", c_dbl), ("dt0", c_dbl),
-                ("max_steps", c_i64)]
+                ("max_steps", c_i64), ("only_flagged", c_i32), ("dense_output", c_i32)]
+
+
+class SurrogateIO(ctypes.Structure):
+    _fields_ = [("nb", c_i64), ("b_first", c_i64), ("nq_t", c_i64), ("t_index", c_vp), ("ld", c_i32)]
+
+
+class SurrogateAccept(ctypes.Structure):
+    _fields_ = [("residual_tol", c_dbl), ("phase_tol", c_dbl), ("pos_err", c_dbl)]
 
 
 class Trajectories(ctypes.Structure):
@@ -90,6 +98,12 @@ SIGNATURES = {
     "msgb_sum_fwd_f32_static": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp]),
     "msgb_rk4_trajectories": (ctypes.c_int, [c_vp, c_vp, c_vp, ctypes.c_int, c_vp, c_vp]),
     "msgb_ode_trajectories": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "msgb_threshold_workspace_size": (c_sz, [c_i64]),
+    "msgb_threshold": (ctypes.c_int, [ctypes.c_int, c_dbl, c_vp, c_vp, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_sz,
+                                      c_vp]),
+    "msgb_surrogate_features": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "msgb_surrogate_targets": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "msgb_surrogate_records": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "msgb_sum_fwd_f64_traj": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp]),
     "msgb_adj_gather_f64_traj": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "msgb_sum_f32_traj_workspace_size": (c_sz, [c_vp, c_i64]),

@@ -16,141 +16,10 @@
 // per save interval).  One thread per beam; the state is written at every
 // acquisition time.  A is integrated from 1 (the equation is linear in A):
 // the summation multiplies by the beam amplitude.
-#include "common.cuh"
+#include "traj.cuh"
 
 namespace msgb {
 namespace {
-
-struct MediumArgs {
-    int kind, boundary;
-    int n[3];
-    double spacing[3], origin[3];
-    const double *coeffs;
-    double c, lam;
-};
-
-__device__ __forceinline__ int map_index(int i, int n, int boundary) {
-    if (n == 1) return 0;
-    switch (boundary) {
-        case 0: return i < 0 ? 0 : (i > n - 1 ? n - 1 : i);
-        case 1: { int r = i % n; return r < 0 ? r + n : r; }
-        case 2: { const int per = 2 * n; int r = i % per; if (r < 0) r += per; return r < n ? r : per - 1 - r; }
-        default: { const int per = 2 * n - 2; int r = i % per; if (r < 0) r += per; return r < n ? r : per - r; }
-    }
-}
-
-// c, grad c (D), hess c (D x D, row-major) at x.
-template <int D>
-__device__ void speed_eval(const MediumArgs &m, const double *x, double &c, double *g, double *H) {
-    if (m.kind == MSGB_MEDIUM_CONSTANT) {
-        c = m.c;
-#pragma unroll
-        for (int i = 0; i < D; ++i) {
-            g[i] = 0.0;
-#pragma unroll
-            for (int k = 0; k < D; ++k) H[i * D + k] = 0.0;
-        }
-        return;
-    }
-    const bool cubic = m.kind == MSGB_MEDIUM_BSPLINE3;
-    const int taps = cubic ? 4 : 2;
-    const int off0 = cubic ? -1 : 0;
-    double w[D][4], d1[D][4], d2[D][4];
-    int idx[D][4];
-#pragma unroll
-    for (int a = 0; a < D; ++a) {
-        const double u = (x[a] - m.origin[a]) / m.spacing[a];
-        const double fl = floor(u);
-        const double t = u - fl;
-        const int i0 = (int)fl;
-        if (cubic) {
-            const double omt = 1.0 - t, t2 = t * t, t3 = t2 * t;
-            w[a][0] = omt * omt * omt / 6.0;
-            w[a][1] = (3.0 * t3 - 6.0 * t2 + 4.0) / 6.0;
-            w[a][2] = (-3.0 * t3 + 3.0 * t2 + 3.0 * t + 1.0) / 6.0;
-            w[a][3] = t3 / 6.0;
-            d1[a][0] = -(omt * omt) / 2.0;
-            d1[a][1] = 1.5 * t2 - 2.0 * t;
-            d1[a][2] = -1.5 * t2 + t + 0.5;
-            d1[a][3] = t2 / 2.0;
-            d2[a][0] = omt;
-            d2[a][1] = 3.0 * t - 2.0;
-            d2[a][2] = -3.0 * t + 1.0;
-            d2[a][3] = t;
-        } else {
-            w[a][0] = 1.0 - t;
-            w[a][1] = t;
-            d1[a][0] = -1.0;
-            d1[a][1] = 1.0;
-            d2[a][0] = d2[a][1] = 0.0;
-            w[a][2] = w[a][3] = d1[a][2] = d1[a][3] = d2[a][2] = d2[a][3] = 0.0;
-        }
-        for (int k = 0; k < taps; ++k) idx[a][k] = map_index(i0 + off0 + k, m.n[a], m.boundary);
-    }
-    double cc = 0.0, gg[D], hh[D][D];
-#pragma unroll
-    for (int i = 0; i < D; ++i) {
-        gg[i] = 0.0;
-#pragma unroll
-        for (int k = 0; k < D; ++k) hh[i][k] = 0.0;
-    }
-    const int ncorner = D == 1 ? taps : (D == 2 ? taps * taps : taps * taps * taps);
-    for (int corner = 0; corner < ncorner; ++corner) {
-        int loc[D];
-        int rem = corner;
-        int64_t flat = 0;
-#pragma unroll
-        for (int a = D - 1; a >= 0; --a) {
-            loc[a] = rem % taps;
-            rem /= taps;
-        }
-#pragma unroll
-        for (int a = 0; a < D; ++a) flat = flat * m.n[a] + idx[a][loc[a]];
-        const double v = __ldg(m.coeffs + flat);
-        double wall = 1.0;
-#pragma unroll
-        for (int a = 0; a < D; ++a) wall *= w[a][loc[a]];
-        cc = fma(wall, v, cc);
-#pragma unroll
-        for (int a = 0; a < D; ++a) {
-            double ga = d1[a][loc[a]];
-            double ha = d2[a][loc[a]];
-#pragma unroll
-            for (int o = 0; o < D; ++o)
-                if (o != a) {
-                    ga *= w[o][loc[o]];
-                    ha *= w[o][loc[o]];
-                }
-            gg[a] = fma(ga, v, gg[a]);
-            hh[a][a] = fma(ha, v, hh[a][a]);
-#pragma unroll
-            for (int b = a + 1; b < D; ++b) {
-                double hab = d1[a][loc[a]] * d1[b][loc[b]];
-#pragma unroll
-                for (int o = 0; o < D; ++o)
-                    if (o != a && o != b) hab *= w[o][loc[o]];
-                hh[a][b] = fma(hab, v, hh[a][b]);
-            }
-        }
-    }
-    c = cc;
-#pragma unroll
-    for (int a = 0; a < D; ++a) {
-        g[a] = gg[a] / m.spacing[a];
-#pragma unroll
-        for (int b = 0; b < D; ++b) {
-            const double hv = a <= b ? hh[a][b] : hh[b][a];
-            H[a * D + b] = hv / (m.spacing[a] * m.spacing[b]);
-        }
-    }
-}
-
-template <int D>
-struct State {
-    double x[D], p[D];
-    cd M[D][D];
-    cd A;
-};
 
 template <int D>
 __device__ void rhs(const MediumArgs &med, double mode, const State<D> &y, State<D> &dy) {
@@ -276,6 +145,7 @@ struct OdeArgs {
     int method, substeps;
     double rtol, atol, dt0;
     int64_t max_steps;
+    int only_flagged, dense_output;
 };
 
 template <int D>
@@ -296,24 +166,62 @@ __device__ __forceinline__ double entry_abs(const double *v, int e) {
     return hypot(v[q], v[q + 1]);
 }
 
-// One adaptive step attempt sequence from t to t_end.  Returns 0, or 2 when
-// the step budget runs out (the state then stays at the last accepted step).
+// Continuous-extension weights (Shampine 1986, the dense output of Hairer,
+// Norsett & Wanner's dopri5): 4th-order interpolant inside an accepted step.
+__constant__ double DP_D[7] = {-12715105075.0 / 11282082432.0, 0.0, 87487479700.0 / 32700410799.0,
+                               -10690763975.0 / 1880347072.0, 701980252875.0 / 199316789632.0,
+                               -1453857185.0 / 822651844.0, 69997945.0 / 29380423.0};
+
+// Adaptive integration of one beam from ts[0] to ts[nt-1], one attempted
+// step per call of attempt(); a step accepted right after a rejection does
+// not grow the next one.  Save times, by o.dense_output:
+//   0: a step that would pass the next save time is shortened to end on it,
+//      and the proposal it replaced is kept for the following step (every
+//      step is at most one save interval long, which also keeps the explicit
+//      method inside its stability region for strongly focusing beams);
+//   1: steps follow the error control alone (only the last is shortened to
+//      end at ts[nt-1]) and save times inside a step are read from the
+//      continuous extension, as diffrax's SaveAt(ts) reads its interpolant.
 template <int D>
-__device__ int dopri_advance(const MediumArgs &med, double mode, State<D> &y, State<D> &f0, double &t,
-                             const double t_end, double &h, int64_t &steps, const OdeArgs &o) {
-    constexpr int N = NV<D>::value;
-    constexpr int NE = 2 * D + D * D + 1;
-    static_assert(sizeof(State<D>) == N * sizeof(double), "State<D> must be a plain array of doubles");
-    while (t < t_end) {
-        if (steps >= o.max_steps) return 2;
-        double hh = h;
-        bool clipped = false;
-        if (t + hh >= t_end) {
-            hh = t_end - t;
-            clipped = true;
+struct DopriBeam {
+    State<D> y, f0;
+    double t, h, mode;
+    int64_t steps, k;
+    bool rejected;
+    int code;  // 0 running or done, 1 non-finite, 2 step budget exhausted
+
+    __device__ void init(const MediumArgs &med, const ProbArgs &P, const OdeArgs &o, double mode_) {
+        mode = mode_;
+        h = o.dt0 > 0.0 ? o.dt0 : (P.nt > 1 ? P.ts[1] - P.ts[0] : 0.0);
+        t = P.ts[0];
+        steps = 0;
+        k = 1;
+        rejected = false;
+        code = 0;
+        rhs<D>(med, mode, y, f0);
+    }
+
+    // One attempt; returns true when the beam is finished (all save times
+    // written or the step budget exhausted).
+    __device__ bool attempt(const MediumArgs &med, const ProbArgs &P, const OdeArgs &o, RecordWriter<D> &rw) {
+        constexpr int N = NV<D>::value;
+        constexpr int NE = 2 * D + D * D + 1;
+        static_assert(sizeof(State<D>) == N * sizeof(double), "State<D> must be a plain array of doubles");
+        if (k >= P.nt) return true;
+        if (steps >= o.max_steps) {
+            code = 2;
+            return true;
         }
-        State<D> k[7];
-        k[0] = f0;
+        const double t_last = P.ts[P.nt - 1];
+        const double target = o.dense_output ? t_last : P.ts[k];
+        double hh = h;
+        bool last = false;
+        if (t + hh >= target) {
+            hh = target - t;
+            last = true;
+        }
+        State<D> kk[7];
+        kk[0] = f0;
         State<D> yt;
         const double *yv = vals(y);
 #pragma unroll 1
@@ -324,82 +232,138 @@ __device__ int dopri_advance(const MediumArgs &med, double mode, State<D> &y, St
                 double acc = 0.0;
                 for (int j = 0; j < s; ++j) {
                     const double a = DP_A[s][j];
-                    if (a != 0.0) acc += a * vals(k[j])[c];
+                    if (a != 0.0) acc += a * vals(kk[j])[c];
                 }
                 tv[c] = yv[c] + hh * acc;
             }
-            rhs<D>(med, mode, yt, k[s]);
+            rhs<D>(med, mode, yt, kk[s]);
         }
         // yt now holds the 5th-order solution (stage 7's input).
-        double ev[N];
-#pragma unroll
-        for (int c = 0; c < N; ++c) {
-            double acc = 0.0;
-            for (int j = 0; j < 7; ++j) acc += DP_E[j] * vals(k[j])[c];
-            ev[c] = hh * acc;
-        }
         double sum = 0.0;
         const double *nv = vals(yt);
+        {
+            double ev[N];
 #pragma unroll
-        for (int e = 0; e < NE; ++e) {
-            const double sc = o.atol + o.rtol * fmax(entry_abs<D>(yv, e), entry_abs<D>(nv, e));
-            const double r = entry_abs<D>(ev, e) / sc;
-            sum += r * r;
+            for (int c = 0; c < N; ++c) {
+                double acc = 0.0;
+                for (int j = 0; j < 7; ++j) acc += DP_E[j] * vals(kk[j])[c];
+                ev[c] = hh * acc;
+            }
+#pragma unroll
+            for (int e = 0; e < NE; ++e) {
+                const double sc = o.atol + o.rtol * fmax(entry_abs<D>(yv, e), entry_abs<D>(nv, e));
+                const double r = entry_abs<D>(ev, e) / sc;
+                sum += r * r;
+            }
         }
         const double err = sqrt(sum / NE);
         ++steps;
         if (!isfinite(err)) {
             h = 0.2 * hh;
-            continue;
+            rejected = true;
+            return false;
         }
-        const double fac = err == 0.0 ? 10.0 : fmin(10.0, fmax(0.2, 0.9 * pow(err, -0.2)));
+        double fac = err == 0.0 ? 10.0 : fmin(10.0, fmax(0.2, 0.9 * pow(err, -0.2)));
         if (err <= 1.0) {
-            t = clipped ? t_end : t + hh;
+            if (rejected) fac = fmin(fac, 1.0);
+            rejected = false;
+            const double t_new = last ? target : t + hh;
+            while (k < P.nt && P.ts[k] <= t_new) {
+                if (P.ts[k] == t_new) {
+                    rw.put(k, yt, false);
+                } else {
+                    const double th = (P.ts[k] - t) / hh;
+                    State<D> yd;
+                    double *dv = vals(yd);
+#pragma unroll
+                    for (int c = 0; c < N; ++c) {
+                        double r5 = 0.0;
+                        for (int j = 0; j < 7; ++j) {
+                            const double dj = DP_D[j];
+                            if (dj != 0.0) r5 += dj * vals(kk[j])[c];
+                        }
+                        r5 *= hh;
+                        const double r2 = nv[c] - yv[c];
+                        const double r3 = hh * vals(kk[0])[c] - r2;
+                        const double r4 = r2 - hh * vals(kk[6])[c] - r3;
+                        dv[c] = yv[c] + th * (r2 + (1.0 - th) * (r3 + th * (r4 + (1.0 - th) * r5)));
+                    }
+                    rw.put(k, yd, false);
+                }
+                ++k;
+            }
+            t = t_new;
             y = yt;
-            f0 = k[6];
-            const double hn = hh * fac;
-            h = clipped ? fmax(hn, h) : hn;
+            f0 = kk[6];
+            h = (last && !o.dense_output) ? fmax(hh * fac, h) : hh * fac;
         } else {
             h = hh * fmin(1.0, fac);
+            rejected = true;
         }
+        return k >= P.nt;
     }
-    return 0;
-}
-
-// Smallest eigenvalue of a symmetric D x D matrix (exact for D <= 2,
-// Gershgorin lower bound for D = 3).
-template <int D>
-__device__ __forceinline__ double lam_min(const double (*S)[D]) {
-    if (D == 1) return S[0][0];
-    if (D == 2) {
-        const double a = S[0][0], b = 0.5 * (S[0][1 % D] + S[1 % D][0]), c = S[1 % D][1 % D];
-        const double m = 0.5 * (a + c), r = sqrt(0.25 * (a - c) * (a - c) + b * b);
-        return m - r;
-    }
-    double lo = 1e300;
-#pragma unroll
-    for (int i = 0; i < D; ++i) {
-        double s = S[i][i];
-#pragma unroll
-        for (int k = 0; k < D; ++k)
-            if (k != i) s -= fabs(0.5 * (S[i][k] + S[k][i]));
-        lo = fmin(lo, s);
-    }
-    return lo;
-}
-
-struct TrajArgs {
-    int64_t nb, b_first, n;
-    double *rec64;
-    void *rec32;
-    float *cull;
-    int32_t *status;
 };
 
 template <int D>
-__global__ void ode_kernel(ProbArgs P, MediumArgs med, BeamArgs B, TrajArgs T, OdeArgs o, int tt_len) {
+__device__ void launch_state(const BeamArgs &B, const TrajArgs &T, int64_t bl, State<D> &y, double &mode, double &w) {
+    const int64_t b = T.b_first + bl;
+    const int64_t j = b < B.n ? b : b - B.n;
+    mode = b < B.n ? 1.0 : -1.0;
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+        y.x[i] = B.x0[j * D + i];
+        y.p[i] = B.p0[j * D + i];
+#pragma unroll
+        for (int k = 0; k < D; ++k) y.M[i][k] = cd{0.0, 0.0};
+        y.M[i][i] = cd{B.alpha[2 * (j * D + i)], B.alpha[2 * (j * D + i) + 1]};
+    }
+    y.A = cd{1.0, 0.0};
+    w = B.omega[j];
+}
+
+// Adaptive integration with persistent lanes: thread i integrates beams
+// i, i + stride, i + 2 stride, ... one attempted step per loop trip, so a
+// lane whose beam finishes early starts its next beam instead of idling
+// until the slowest beam of its warp is done.
+template <int D>
+__global__ void dopri_kernel(ProbArgs P, MediumArgs med, BeamArgs B, TrajArgs T, OdeArgs o, int tt_len) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t bl = blockIdx.x * (int64_t)blockDim.x + threadIdx.x - stride;
+    bool active = false;
+    DopriBeam<D> s;
+    RecordWriter<D> rw(P, T, 0, 0.0, tt_len);
+    for (;;) {
+        if (!active) {
+            bl += stride;
+            while (bl < T.nb && o.only_flagged && T.status[bl] == 0) bl += stride;  // already accepted
+            if (bl < T.nb) {
+                double mode, w;
+                launch_state<D>(B, T, bl, s.y, mode, w);
+                rw.reset(bl, w);
+                rw.put(0, s.y, false);
+                s.init(med, P, o, mode);
+                active = true;
+            }
+        }
+        if (!__any_sync(0xffffffffu, active)) break;
+        if (active && s.attempt(med, P, o, rw)) {
+            bool fin = isfinite(s.y.A.re) && isfinite(s.y.A.im);
+#pragma unroll
+            for (int i = 0; i < D; ++i) fin = fin && isfinite(s.y.x[i]) && isfinite(s.y.p[i]);
+            if (!fin && s.code == 0) s.code = 1;
+            for (int64_t k = s.k; k < P.nt; ++k) rw.put(k, s.y, true);  // after a failure: last state
+            if (T.status) T.status[bl] = s.code;
+            active = false;
+        }
+    }
+}
+
+// Fixed-step RK4, one thread per beam.
+template <int D>
+__global__ void rk4_kernel(ProbArgs P, MediumArgs med, BeamArgs B, TrajArgs T, OdeArgs o, int tt_len) {
     const int64_t bl = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (bl >= T.nb) return;
+    if (o.only_flagged && T.status[bl] == 0) return;  // records already accepted
     const int64_t b = T.b_first + bl;
     const int64_t j = b < B.n ? b : b - B.n;
     const double mode = b < B.n ? 1.0 : -1.0;
@@ -414,109 +378,19 @@ __global__ void ode_kernel(ProbArgs P, MediumArgs med, BeamArgs B, TrajArgs T, O
     }
     y.A = cd{1.0, 0.0};
     const double w = B.omega[j];
-    const bool adaptive = o.method == MSGB_ODE_DOPRI5;
-    double h = o.dt0 > 0.0 ? o.dt0 : (P.nt > 1 ? P.ts[1] - P.ts[0] : 0.0);
-    double t = P.ts[0];
-    int64_t steps = 0;
     int code = 0;
-    State<D> f0;
-    if (adaptive) rhs<D>(med, mode, y, f0);
-    constexpr int S = D * (D + 1) / 2;
-    constexpr int NR64 = 2 * D + 2 * D * D + 2;
-    float lo[D], hi[D];
-    double lmin = 1e300;
-    bool bad = false;
+    RecordWriter<D> rw(P, T, bl, w, tt_len);
     const int64_t n_tt = (P.nt + tt_len - 1) / tt_len;
     for (int64_t k = 0; k < P.nt; ++k) {
         if (k > 0 && code == 0) {
-            if (adaptive) {
-                code = dopri_advance<D>(med, mode, y, f0, t, P.ts[k], h, steps, o);
-            } else {
-                const double hs = (P.ts[k] - P.ts[k - 1]) / o.substeps;
-                for (int s = 0; s < o.substeps; ++s) rk4_step<D>(med, mode, y, hs);
-            }
+            const double hs = (P.ts[k] - P.ts[k - 1]) / o.substeps;
+            for (int s = 0; s < o.substeps; ++s) rk4_step<D>(med, mode, y, hs);
         }
         bool fin = isfinite(y.A.re) && isfinite(y.A.im);
 #pragma unroll
         for (int i = 0; i < D; ++i) fin = fin && isfinite(y.x[i]) && isfinite(y.p[i]);
         if (!fin && code == 0) code = 1;
-        bad |= code != 0;
-        double xw[D];
-#pragma unroll
-        for (int i = 0; i < D; ++i) xw[i] = P.periodic[i] ? pymod(y.x[i], P.L[i]) : y.x[i];
-        if (T.rec64) {
-            double *r = T.rec64 + (k * T.nb + bl) * NR64;
-            int q = 0;
-#pragma unroll
-            for (int i = 0; i < D; ++i) r[q++] = y.x[i];
-#pragma unroll
-            for (int i = 0; i < D; ++i) r[q++] = y.p[i];
-#pragma unroll
-            for (int i = 0; i < D; ++i)
-#pragma unroll
-                for (int l = 0; l < D; ++l) {
-                    r[q++] = y.M[i][l].re;
-                    r[q++] = y.M[i][l].im;
-                }
-            r[q++] = y.A.re;
-            r[q++] = y.A.im;
-        }
-        if (T.rec32) {
-            // layout of the FP32 summation's BeamTime<D> record
-            char *base = (char *)T.rec32 + (k * T.nb + bl) * (int64_t)(16 * D + 8 * S + 8);
-            double *xd = (double *)base;
-            double *wpd = xd + D;
-            float *f = (float *)(wpd + D);
-#pragma unroll
-            for (int i = 0; i < D; ++i) {
-                xd[i] = xw[i];
-                wpd[i] = w * y.p[i];
-            }
-#pragma unroll
-            for (int i = 0; i < D; ++i)
-#pragma unroll
-                for (int l = i; l < D; ++l) {
-                    const int q = sym_index<D>(i, l);
-                    const double fac = (i == l ? 0.5 : 0.5) * w;  // off-diagonal: (M_il + M_li)/2 doubled
-                    const double mre = i == l ? y.M[i][i].re : (y.M[i][l].re + y.M[l][i].re);
-                    const double mim = i == l ? y.M[i][i].im : (y.M[i][l].im + y.M[l][i].im);
-                    f[q] = (float)(fac * mre);
-                    f[S + q] = (float)(fac * mim);
-                }
-            f[2 * S] = (float)atan2(y.A.im, (y.A.re == 0.0 && y.A.im == 0.0) ? 1e-12 : y.A.re);
-            f[2 * S + 1] = (float)(2.0 * hypot(y.A.re, y.A.im));
-        }
-        if (T.cull) {
-            double Sm[D][D];
-#pragma unroll
-            for (int i = 0; i < D; ++i)
-#pragma unroll
-                for (int l = 0; l < D; ++l) Sm[i][l] = y.M[i][l].im;
-            const int kk = (int)(k % tt_len);
-            if (kk == 0) {
-                lmin = 1e300;
-#pragma unroll
-                for (int i = 0; i < D; ++i) lo[i] = 3.4e38f, hi[i] = -3.4e38f;
-            }
-            lmin = fmin(lmin, lam_min<D>(Sm));
-#pragma unroll
-            for (int i = 0; i < D; ++i) {
-                const float xf = (float)xw[i];
-                lo[i] = fminf(lo[i], xf);
-                hi[i] = fmaxf(hi[i], xf);
-            }
-            if (kk == tt_len - 1 || k == P.nt - 1) {
-                float *c = T.cull + ((k / tt_len) * T.nb + bl) * (2 * D + 1);
-#pragma unroll
-                for (int i = 0; i < D; ++i) {
-                    // periodic axes and non-finite states are never culled
-                    const bool open = P.periodic[i] || bad;
-                    c[i] = open ? -3.4e38f : lo[i];
-                    c[D + i] = open ? 3.4e38f : hi[i];
-                }
-                c[2 * D] = bad ? 0.0f : (float)fmax(0.0, 0.5 * w * lmin * (1.0 - 1e-6));
-            }
-        }
+        rw.put(k, y, code != 0);
     }
     (void)n_tt;
     if (T.status) T.status[bl] = code;
@@ -546,38 +420,37 @@ extern "C" int msgb_ode_trajectories(const msgb_problem *prob, const msgb_medium
     if (out->nb < 0 || out->b_first < 0 || out->b_first + out->nb > 2 * beams->n)
         return fail(MSGB_ERR_ARG, "beam range [%lld, %lld) outside [0, 2n)", (long long)out->b_first,
                     (long long)(out->b_first + out->nb));
-    if (med->kind != MSGB_MEDIUM_CONSTANT) {
-        if (med->kind != MSGB_MEDIUM_LINEAR && med->kind != MSGB_MEDIUM_BSPLINE3)
-            return fail(MSGB_ERR_ARG, "unknown medium kind %d", med->kind);
-        if (!med->coeffs) return fail(MSGB_ERR_ARG, "medium grid is NULL");
-        if (med->boundary < 0 || med->boundary > 3) return fail(MSGB_ERR_ARG, "unknown boundary %d", med->boundary);
-        for (int a = 0; a < prob->ndim; ++a)
-            if (med->n[a] < 1 || !(med->spacing[a] > 0.0)) return fail(MSGB_ERR_ARG, "bad medium grid");
-    } else if (!(med->c > 0.0)) {
-        return fail(MSGB_ERR_ARG, "constant medium speed must be > 0");
-    }
+    MediumArgs M;
+    if (int e = medium_args(prob, med, M)) return e;
     if (out->nb == 0 || prob->nt == 0) return MSGB_OK;
+    if (opts->only_flagged && !out->status)
+        return fail(MSGB_ERR_ARG, "only_flagged needs the status array of the records");
     ProbArgs P = to_args(prob);
-    MediumArgs M{};
-    M.kind = med->kind;
-    M.boundary = med->boundary;
-    for (int a = 0; a < 3; ++a) {
-        M.n[a] = med->n[a];
-        M.spacing[a] = med->spacing[a];
-        M.origin[a] = med->origin[a];
-    }
-    M.coeffs = med->coeffs;
-    M.c = med->c;
-    M.lam = med->lam;
-    OdeArgs O{opts->method, opts->substeps, opts->rtol, opts->atol, opts->dt0, opts->max_steps};
+    OdeArgs O{opts->method, opts->substeps, opts->rtol, opts->atol, opts->dt0, opts->max_steps, opts->only_flagged,
+              opts->dense_output};
     TrajArgs T{out->nb, out->b_first, beams->n, out->rec64, out->rec32, out->cull, out->status};
     const int blk = 64;
-    const unsigned grid = (unsigned)((out->nb + blk - 1) / blk);
+    const int64_t need = (out->nb + blk - 1) / blk;
     cudaStream_t st = as_stream(stream);
-    switch (prob->ndim) {
-        case 1: ode_kernel<1><<<grid, blk, 0, st>>>(P, M, to_args(beams), T, O, MSGB_TIME_TILE); break;
-        case 2: ode_kernel<2><<<grid, blk, 0, st>>>(P, M, to_args(beams), T, O, MSGB_TIME_TILE); break;
-        default: ode_kernel<3><<<grid, blk, 0, st>>>(P, M, to_args(beams), T, O, MSGB_TIME_TILE); break;
+    if (O.method == MSGB_ODE_RK4) {
+        const unsigned grid = (unsigned)need;
+        switch (prob->ndim) {
+            case 1: rk4_kernel<1><<<grid, blk, 0, st>>>(P, M, to_args(beams), T, O, MSGB_TIME_TILE); break;
+            case 2: rk4_kernel<2><<<grid, blk, 0, st>>>(P, M, to_args(beams), T, O, MSGB_TIME_TILE); break;
+            default: rk4_kernel<3><<<grid, blk, 0, st>>>(P, M, to_args(beams), T, O, MSGB_TIME_TILE); break;
+        }
+    } else {
+        // enough resident lanes for every SM, each taking several beams
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const int64_t want = 4LL * sms;
+        const unsigned grid = (unsigned)(need < want ? need : want);
+        switch (prob->ndim) {
+            case 1: dopri_kernel<1><<<grid, blk, 0, st>>>(P, M, to_args(beams), T, O, MSGB_TIME_TILE); break;
+            case 2: dopri_kernel<2><<<grid, blk, 0, st>>>(P, M, to_args(beams), T, O, MSGB_TIME_TILE); break;
+            default: dopri_kernel<3><<<grid, blk, 0, st>>>(P, M, to_args(beams), T, O, MSGB_TIME_TILE); break;
+        }
     }
     return check_launch("msgb_ode_trajectories");
 }

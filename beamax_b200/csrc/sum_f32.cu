@@ -812,19 +812,33 @@ adj32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
                                 gq += CH;
                                 continue;
                             }
+                            float d1[CH], ar[CH], ai[CH];
+#pragma unroll
+                            for (int c = 0; c < CH; ++c) {
+                                d1[c] = tv ? __ldg(dcol + (int64_t)((gq + c) * GS + 1) * P.nt) : 0.0f;
+                                ar[c] = 0.0f;
+                                ai[c] = 0.0f;
+                            }
+#pragma unroll 4
                             for (int kk = 0; kk < GS; ++kk) {
                                 float dn[CH];
 #pragma unroll
                                 for (int c = 0; c < CH; ++c)
-                                    dn[c] = (tv && kk + 1 < GS) ? __ldg(dcol + (int64_t)((gq + c) * GS + kk + 1) * P.nt) : 0.0f;
+                                    dn[c] = (tv && kk + 2 < GS) ? __ldg(dcol + (int64_t)((gq + c) * GS + kk + 2) * P.nt) : 0.0f;
 #pragma unroll
                                 for (int c = 0; c < CH; ++c) {
-                                    pr = fmaf(d[c], z[c].re, pr);
-                                    pi = fmaf(-d[c], z[c].im, pi);
+                                    ar[c] = fmaf(d[c], z[c].re, ar[c]);
+                                    ai[c] = fmaf(-d[c], z[c].im, ai[c]);
                                     z[c] = cmul(z[c], rr[c]);
                                     rr[c] = cmul(rr[c], qq[c]);
-                                    d[c] = dn[c];
+                                    d[c] = d1[c];
+                                    d1[c] = dn[c];
                                 }
+                            }
+#pragma unroll
+                            for (int c = 0; c < CH; ++c) {
+                                pr += ar[c];
+                                pi += ai[c];
                             }
                             gq += CH;
                         } else {

@@ -1,0 +1,315 @@
+// Shared by the beam ODE (rk4.cu) and the trajectory surrogate (surrogate.cu):
+// the sound speed interpolant with its derivatives, the beam state, and the
+// writer of trajectory records (FP64 records, FP32 summation records, and the
+// per-time-tile culling boxes) in the layout msgb_trajectories documents.
+#pragma once
+
+#include "common.cuh"
+
+namespace msgb {
+namespace {
+
+struct MediumArgs {
+    int kind, boundary;
+    int n[3];
+    double spacing[3], origin[3];
+    const double *coeffs;
+    double c, lam;
+};
+
+__device__ __forceinline__ int map_index(int i, int n, int boundary) {
+    if (n == 1) return 0;
+    switch (boundary) {
+        case 0: return i < 0 ? 0 : (i > n - 1 ? n - 1 : i);
+        case 1: { int r = i % n; return r < 0 ? r + n : r; }
+        case 2: { const int per = 2 * n; int r = i % per; if (r < 0) r += per; return r < n ? r : per - 1 - r; }
+        default: { const int per = 2 * n - 2; int r = i % per; if (r < 0) r += per; return r < n ? r : per - r; }
+    }
+}
+
+// c, grad c (D), hess c (D x D, row-major) at x.
+template <int D>
+__device__ void speed_eval(const MediumArgs &m, const double *x, double &c, double *g, double *H) {
+    if (m.kind == MSGB_MEDIUM_CONSTANT) {
+        c = m.c;
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+            g[i] = 0.0;
+#pragma unroll
+            for (int k = 0; k < D; ++k) H[i * D + k] = 0.0;
+        }
+        return;
+    }
+    const bool cubic = m.kind == MSGB_MEDIUM_BSPLINE3;
+    const int taps = cubic ? 4 : 2;
+    const int off0 = cubic ? -1 : 0;
+    double w[D][4], d1[D][4], d2[D][4];
+    int idx[D][4];
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        const double u = (x[a] - m.origin[a]) / m.spacing[a];
+        const double fl = floor(u);
+        const double t = u - fl;
+        const int i0 = (int)fl;
+        if (cubic) {
+            const double omt = 1.0 - t, t2 = t * t, t3 = t2 * t;
+            w[a][0] = omt * omt * omt / 6.0;
+            w[a][1] = (3.0 * t3 - 6.0 * t2 + 4.0) / 6.0;
+            w[a][2] = (-3.0 * t3 + 3.0 * t2 + 3.0 * t + 1.0) / 6.0;
+            w[a][3] = t3 / 6.0;
+            d1[a][0] = -(omt * omt) / 2.0;
+            d1[a][1] = 1.5 * t2 - 2.0 * t;
+            d1[a][2] = -1.5 * t2 + t + 0.5;
+            d1[a][3] = t2 / 2.0;
+            d2[a][0] = omt;
+            d2[a][1] = 3.0 * t - 2.0;
+            d2[a][2] = -3.0 * t + 1.0;
+            d2[a][3] = t;
+        } else {
+            w[a][0] = 1.0 - t;
+            w[a][1] = t;
+            d1[a][0] = -1.0;
+            d1[a][1] = 1.0;
+            d2[a][0] = d2[a][1] = 0.0;
+            w[a][2] = w[a][3] = d1[a][2] = d1[a][3] = d2[a][2] = d2[a][3] = 0.0;
+        }
+        for (int k = 0; k < taps; ++k) idx[a][k] = map_index(i0 + off0 + k, m.n[a], m.boundary);
+    }
+    double cc = 0.0, gg[D], hh[D][D];
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+        gg[i] = 0.0;
+#pragma unroll
+        for (int k = 0; k < D; ++k) hh[i][k] = 0.0;
+    }
+    const int ncorner = D == 1 ? taps : (D == 2 ? taps * taps : taps * taps * taps);
+    for (int corner = 0; corner < ncorner; ++corner) {
+        int loc[D];
+        int rem = corner;
+        int64_t flat = 0;
+#pragma unroll
+        for (int a = D - 1; a >= 0; --a) {
+            loc[a] = rem % taps;
+            rem /= taps;
+        }
+#pragma unroll
+        for (int a = 0; a < D; ++a) flat = flat * m.n[a] + idx[a][loc[a]];
+        const double v = __ldg(m.coeffs + flat);
+        double wall = 1.0;
+#pragma unroll
+        for (int a = 0; a < D; ++a) wall *= w[a][loc[a]];
+        cc = fma(wall, v, cc);
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+            double ga = d1[a][loc[a]];
+            double ha = d2[a][loc[a]];
+#pragma unroll
+            for (int o = 0; o < D; ++o)
+                if (o != a) {
+                    ga *= w[o][loc[o]];
+                    ha *= w[o][loc[o]];
+                }
+            gg[a] = fma(ga, v, gg[a]);
+            hh[a][a] = fma(ha, v, hh[a][a]);
+#pragma unroll
+            for (int b = a + 1; b < D; ++b) {
+                double hab = d1[a][loc[a]] * d1[b][loc[b]];
+#pragma unroll
+                for (int o = 0; o < D; ++o)
+                    if (o != a && o != b) hab *= w[o][loc[o]];
+                hh[a][b] = fma(hab, v, hh[a][b]);
+            }
+        }
+    }
+    c = cc;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        g[a] = gg[a] / m.spacing[a];
+#pragma unroll
+        for (int b = 0; b < D; ++b) {
+            const double hv = a <= b ? hh[a][b] : hh[b][a];
+            H[a * D + b] = hv / (m.spacing[a] * m.spacing[b]);
+        }
+    }
+}
+
+template <int D>
+struct State {
+    double x[D], p[D];
+    cd M[D][D];
+    cd A;
+};
+
+// Smallest eigenvalue of a symmetric D x D matrix (exact for D <= 2,
+// Gershgorin lower bound for D = 3).
+template <int D>
+__device__ __forceinline__ double lam_min(const double (*S)[D]) {
+    if (D == 1) return S[0][0];
+    if (D == 2) {
+        const double a = S[0][0], b = 0.5 * (S[0][1 % D] + S[1 % D][0]), c = S[1 % D][1 % D];
+        const double m = 0.5 * (a + c), r = sqrt(0.25 * (a - c) * (a - c) + b * b);
+        return m - r;
+    }
+    double lo = 1e300;
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+        double s = S[i][i];
+#pragma unroll
+        for (int k = 0; k < D; ++k)
+            if (k != i) s -= fabs(0.5 * (S[i][k] + S[k][i]));
+        lo = fmin(lo, s);
+    }
+    return lo;
+}
+
+struct TrajArgs {
+    int64_t nb, b_first, n;
+    double *rec64;
+    void *rec32;
+    float *cull;
+    int32_t *status;
+};
+
+
+// Writes the records of one beam (index bl within the chunk) at every time k,
+// and the culling box of each time tile as its last time is written.
+template <int D>
+struct RecordWriter {
+    static constexpr int S = D * (D + 1) / 2;
+    static constexpr int NR64 = 2 * D + 2 * D * D + 2;
+    const ProbArgs &P;
+    const TrajArgs &T;
+    int64_t bl;
+    double w;
+    int tt_len;
+    float lo[D], hi[D];
+    double lmin = 1e300;
+    bool bad = false;
+
+    __device__ RecordWriter(const ProbArgs &P_, const TrajArgs &T_, int64_t bl_, double w_, int tt_len_)
+        : P(P_), T(T_), bl(bl_), w(w_), tt_len(tt_len_) {
+#pragma unroll
+        for (int i = 0; i < D; ++i) lo[i] = 3.4e38f, hi[i] = -3.4e38f;
+    }
+
+    // Start the records of another beam of the same chunk.
+    __device__ void reset(int64_t bl_, double w_) {
+        bl = bl_;
+        w = w_;
+        lmin = 1e300;
+        bad = false;
+#pragma unroll
+        for (int i = 0; i < D; ++i) lo[i] = 3.4e38f, hi[i] = -3.4e38f;
+    }
+
+    // `failed`: the state is not trustworthy from here on (never culled).
+    __device__ void put(int64_t k, const State<D> &y, bool failed) {
+        bad |= failed;
+        double xw[D];
+#pragma unroll
+        for (int i = 0; i < D; ++i) xw[i] = P.periodic[i] ? pymod(y.x[i], P.L[i]) : y.x[i];
+        if (T.rec64) {
+            double *r = T.rec64 + (k * T.nb + bl) * NR64;
+            int q = 0;
+#pragma unroll
+            for (int i = 0; i < D; ++i) r[q++] = y.x[i];
+#pragma unroll
+            for (int i = 0; i < D; ++i) r[q++] = y.p[i];
+#pragma unroll
+            for (int i = 0; i < D; ++i)
+#pragma unroll
+                for (int l = 0; l < D; ++l) {
+                    r[q++] = y.M[i][l].re;
+                    r[q++] = y.M[i][l].im;
+                }
+            r[q++] = y.A.re;
+            r[q++] = y.A.im;
+        }
+        if (T.rec32) {
+            // layout of the FP32 summation's BeamTime<D> record
+            char *base = (char *)T.rec32 + (k * T.nb + bl) * (int64_t)(16 * D + 8 * S + 8);
+            double *xd = (double *)base;
+            double *wpd = xd + D;
+            float *f = (float *)(wpd + D);
+#pragma unroll
+            for (int i = 0; i < D; ++i) {
+                xd[i] = xw[i];
+                wpd[i] = w * y.p[i];
+            }
+#pragma unroll
+            for (int i = 0; i < D; ++i)
+#pragma unroll
+                for (int l = i; l < D; ++l) {
+                    const int q = sym_index<D>(i, l);
+                    const double fac = (i == l ? 0.5 : 0.5) * w;  // off-diagonal: (M_il + M_li)/2 doubled
+                    const double mre = i == l ? y.M[i][i].re : (y.M[i][l].re + y.M[l][i].re);
+                    const double mim = i == l ? y.M[i][i].im : (y.M[i][l].im + y.M[l][i].im);
+                    f[q] = (float)(fac * mre);
+                    f[S + q] = (float)(fac * mim);
+                }
+            f[2 * S] = (float)atan2(y.A.im, (y.A.re == 0.0 && y.A.im == 0.0) ? 1e-12 : y.A.re);
+            f[2 * S + 1] = (float)(2.0 * hypot(y.A.re, y.A.im));
+        }
+        if (T.cull) {
+            double Sm[D][D];
+#pragma unroll
+            for (int i = 0; i < D; ++i)
+#pragma unroll
+                for (int l = 0; l < D; ++l) Sm[i][l] = y.M[i][l].im;
+            const int kk = (int)(k % tt_len);
+            if (kk == 0) {
+                lmin = 1e300;
+#pragma unroll
+                for (int i = 0; i < D; ++i) lo[i] = 3.4e38f, hi[i] = -3.4e38f;
+            }
+            lmin = fmin(lmin, lam_min<D>(Sm));
+#pragma unroll
+            for (int i = 0; i < D; ++i) {
+                const float xf = (float)xw[i];
+                lo[i] = fminf(lo[i], xf);
+                hi[i] = fmaxf(hi[i], xf);
+            }
+            if (kk == tt_len - 1 || k == P.nt - 1) {
+                float *c = T.cull + ((k / tt_len) * T.nb + bl) * (2 * D + 1);
+#pragma unroll
+                for (int i = 0; i < D; ++i) {
+                    // periodic axes and non-finite states are never culled
+                    const bool open = P.periodic[i] || bad;
+                    c[i] = open ? -3.4e38f : lo[i];
+                    c[D + i] = open ? 3.4e38f : hi[i];
+                }
+                c[2 * D] = bad ? 0.0f : (float)fmax(0.0, 0.5 * w * lmin * (1.0 - 1e-6));
+            }
+        }
+    }
+};
+
+// Host: medium description -> kernel arguments (MSGB_OK or an error code).
+inline int medium_args(const msgb_problem *prob, const msgb_medium *med, MediumArgs &M) {
+    if (!med) return fail(MSGB_ERR_ARG, "medium is NULL");
+    if (med->kind != MSGB_MEDIUM_CONSTANT) {
+        if (med->kind != MSGB_MEDIUM_LINEAR && med->kind != MSGB_MEDIUM_BSPLINE3)
+            return fail(MSGB_ERR_ARG, "unknown medium kind %d", med->kind);
+        if (!med->coeffs) return fail(MSGB_ERR_ARG, "medium grid is NULL");
+        if (med->boundary < 0 || med->boundary > 3) return fail(MSGB_ERR_ARG, "unknown boundary %d", med->boundary);
+        for (int a = 0; a < prob->ndim; ++a)
+            if (med->n[a] < 1 || !(med->spacing[a] > 0.0)) return fail(MSGB_ERR_ARG, "bad medium grid");
+    } else if (!(med->c > 0.0)) {
+        return fail(MSGB_ERR_ARG, "constant medium speed must be > 0");
+    }
+    M = MediumArgs{};
+    M.kind = med->kind;
+    M.boundary = med->boundary;
+    for (int a = 0; a < 3; ++a) {
+        M.n[a] = med->n[a];
+        M.spacing[a] = med->spacing[a];
+        M.origin[a] = med->origin[a];
+    }
+    M.coeffs = med->coeffs;
+    M.c = med->c;
+    M.lam = med->lam;
+    return MSGB_OK;
+}
+
+}  // namespace
+}  // namespace msgb

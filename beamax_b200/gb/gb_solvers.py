@@ -79,7 +79,11 @@ class SolverConfig:
     controller is the integral controller the reference's default
     coefficients select (pcoeff 0, icoeff 1, dcoeff 0); other coefficients are
     rejected.  ``substeps`` (no reference counterpart) is the number of RK4
-    steps per save interval.
+    steps per save interval.  ``dense_output`` (no reference counterpart):
+    False ends adaptive steps on every save time (at most one save interval
+    per step, robust for strongly focusing beams); True lets steps follow the
+    error control and reads save times from the continuous extension, as
+    diffrax's SaveAt(ts) does.
     """
 
     solver: Any = "tsit5"
@@ -91,6 +95,7 @@ class SolverConfig:
     dcoeff: float = 0.0
     dt0: Optional[float] = None
     substeps: int = 1
+    dense_output: bool = False
 
     def __post_init__(self) -> None:
         if isinstance(self.max_steps, bool) or not isinstance(self.max_steps, int):

@@ -23,6 +23,7 @@ arguments, msgb_solver.py:1235-1386) is a different operator and raises
 
 from __future__ import annotations
 
+import contextlib
 import ctypes
 import math
 from dataclasses import dataclass
@@ -100,12 +101,15 @@ class MSGBSolver:
         "rk4" (overrides ``ode_config.substeps`` when > 1).
       trajectory_memory: bytes of device memory for trajectory records; beams
         are propagated and summed in chunks that fit.
+      surrogate: a fitted ``beamax_b200.surrogate.TrajectorySurrogate`` for the
+        medium and time grid; heterogeneous beams are predicted by it and the
+        ones it does not accept are integrated.
     """
 
     def __init__(self, thr, thr_strat: str, batch_size: int, input_type: str, ode_solver, sum_method: str,
                  tr_ode_solver=None, sharding=None, ode_config=None, adjoint_relative_guard: float = 5e-2,
                  *, precision: str = "fp64", cutoff: float = 16.0, rk4_substeps: int = 1,
-                 trajectory_memory: int = 16 << 30):
+                 trajectory_memory: int = 16 << 30, surrogate=None):
         valid_thresholds = {"hard", "top_n", "percentile", "hard_reassign", "bao_energy", "perc_max_abs"}
         if thr_strat not in valid_thresholds:
             raise ValueError(f"thr_strat must be one of {', '.join(sorted(valid_thresholds))}; got {thr_strat!r}.")
@@ -163,6 +167,13 @@ class MSGBSolver:
             raise ValueError("rk4_substeps must be a positive integer.")
         self.rk4_substeps = max(int(rk4_substeps), ode_config.substeps)
         self.trajectory_memory = int(trajectory_memory)
+        self.surrogate = surrogate
+        # When set to a list, every FP32 summation entry point call appends
+        # (name, start event, end event, evaluation counter) recorded on the
+        # launching stream around the call.
+        self.kernel_timer = None
+        self.last_surrogate_accepted: Optional[int] = None
+        self._accepted = None
         self.last_selection: Optional[Selection] = None
         self.last_eval_count: Optional[int] = None
 
@@ -238,11 +249,9 @@ class MSGBSolver:
 
     # ------------------------------------------------------------- pipeline
     def select(self, p0, domain: Domain, wpt: MSWPT, dpdt=None) -> Selection:
-        """c_pos on the GPU, then top_n (msgb_solver.py:570-612)."""
+        """c_pos on the GPU, then the threshold (msgb_solver.py:570-612)."""
         import torch
 
-        if self.thr_strat != "top_n":
-            raise NotImplementedError(f"thr_strat={self.thr_strat!r}: only top_n runs on the GPU path")
         x = as_device_f64(p0)
         if x.is_complex():
             raise NotImplementedError("complex p0 (the *_complex parameter path) is not implemented")
@@ -252,6 +261,8 @@ class MSGBSolver:
             if nonzero:
                 raise NotImplementedError("non-zero dpdt is not implemented on the GPU path")
         coeffs, keys = wpt.forward_device(x, self.input_type, scale=0.5, half_mask=True, keys=True)
+        if self.thr_strat != "top_n":
+            return self._select_masked(coeffs, keys, wpt, x.device)
         n = self._effective_top_n(wpt, half_frame=True)
         dev = x.device
         idx = torch.empty(n, dtype=torch.int64, device=dev)
@@ -263,6 +274,28 @@ class MSGBSolver:
                                         n, idx.data_ptr(), torch.view_as_real(vals).data_ptr(), ws.data_ptr(),
                                         nbytes, st), "msgb_topn")
         return Selection(idx, vals, wpt.total_coeffs)
+
+    _THR_CODE = {"hard": 0, "percentile": 1, "hard_reassign": 2, "bao_energy": 3, "perc_max_abs": 4}
+
+    def _select_masked(self, coeffs, keys, wpt: MSWPT, dev) -> Selection:
+        """hard / percentile / hard_reassign / bao_energy / perc_max_abs
+        (forward_solver_utils.py:14-178) via msgb_threshold; one device-to-host
+        read of the selected count."""
+        import torch
+
+        total = wpt.total_coeffs
+        idx = torch.empty(total, dtype=torch.int64, device=dev)
+        vals = torch.empty(total, dtype=torch.complex128, device=dev)
+        count = torch.zeros(1, dtype=torch.int64, device=dev)
+        nbytes = _lib.lib().msgb_threshold_workspace_size(total)
+        ws = workspace(dev, "threshold", nbytes)
+        st = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(_lib.lib().msgb_threshold(self._THR_CODE[self.thr_strat], float(self.thr), keys.data_ptr(),
+                                             torch.view_as_real(coeffs).data_ptr(), total, wpt.plan(dev),
+                                             idx.data_ptr(), torch.view_as_real(vals).data_ptr(), count.data_ptr(),
+                                             ws.data_ptr(), nbytes, st), "msgb_threshold")
+        n = int(count.item())
+        return Selection(idx[:n].clone(), vals[:n].clone(), total)
 
     def beams(self, sel: Selection, domain: Domain, wpt: MSWPT) -> BeamTensors:
         """Beam data for a selection (compute_forward_parameters, a0 *= coefficient)."""
@@ -328,7 +361,8 @@ class MSGBSolver:
         if cfg.method == "rk4":
             return _lib.OdeOpts(method=0, substeps=self.rk4_substeps)
         return _lib.OdeOpts(method=1, substeps=1, rtol=float(cfg.rtol), atol=float(cfg.atol),
-                            dt0=float(cfg.dt0) if cfg.dt0 is not None else 0.0, max_steps=int(cfg.max_steps))
+                            dt0=float(cfg.dt0) if cfg.dt0 is not None else 0.0, max_steps=int(cfg.max_steps),
+                            dense_output=int(bool(cfg.dense_output)))
 
     def _trajectories(self, pr, med, bs, b_first, nb, fp64, per, n_tt, dev, st, status):
         buf = workspace(dev, "traj", per * nb + 4096)
@@ -341,12 +375,38 @@ class MSGBSolver:
                                cull=None if fp64 else base + cull_off,
                                status=status.data_ptr() + 4 * b_first)
         opts = self._ode_opts(None)
+        if self.surrogate is not None:
+            self.surrogate.predict_into(pr, med, bs, b_first, nb, tr)
+            acc = (status[b_first:b_first + nb] == 0).sum()
+            self._accepted = acc if self._accepted is None else self._accepted + acc
+            opts.only_flagged = 1
         _lib.check(_lib.lib().msgb_ode_trajectories(_lib.ref(pr), _lib.ref(med), _lib.ref(bs), _lib.ref(opts),
                                                     _lib.ref(tr), st), "msgb_ode_trajectories")
         return tr, buf
 
+    def _begin_trajectories(self, domain, ts):
+        self._accepted = None
+        if self.surrogate is not None:
+            if getattr(self.surrogate, "_key", None) != self.surrogate.medium_key(domain, ts):
+                raise ValueError("the surrogate was fitted for another medium or time grid")
+
+    @contextlib.contextmanager
+    def _kernel_span(self, name, counter):
+        if self.kernel_timer is None:
+            yield
+            return
+        import torch
+
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        yield
+        b.record()
+        self.kernel_timer.append((name, a, b, counter))
+
     def _check_status(self, status):
         """Raise, as the reference's diffeqsolve does, when an integration failed."""
+        if self.surrogate is not None:
+            self.last_surrogate_accepted = int(self._accepted.item()) if self._accepted is not None else 0
         worst = int(status.max().item()) if status.numel() else 0
         if worst == 2:
             n = int((status == 2).sum().item())
@@ -368,6 +428,7 @@ class MSGBSolver:
         fp64 = self.precision == "fp64"
         chunks, per, n_tt = self._chunks(domain, pr.nt, 2 * bt.n, fp64)
         status = torch.zeros(2 * bt.n, dtype=torch.int32, device=dev)
+        self._begin_trajectories(domain, ts)
         if fp64:
             out = torch.zeros((pr.nt, pr.ns), dtype=torch.float64, device=dev)
             for b_first, nb in chunks:
@@ -417,6 +478,7 @@ class MSGBSolver:
         nbytes = 0 if fp64 else _lib.lib().msgb_sum_f32_traj_workspace_size(_lib.ref(pr), 2 * n)
         ws = None if fp64 else workspace(dev, "sum32traj", nbytes)
         status = torch.zeros(2 * n, dtype=torch.int32, device=dev)
+        self._begin_trajectories(domain, ts)
         for b_first, nb in chunks:
             tr, _ = self._trajectories(pr, med, bs, b_first, nb, fp64, per, n_tt, dev, st, status)
             gp = torch.view_as_real(g_all[b_first:b_first + nb]).data_ptr()
@@ -454,8 +516,9 @@ class MSGBSolver:
                             tiling=_lib.ref(tiling[0]) if tiling else None)
         nbytes = _lib.lib().msgb_sum_f32_workspace_size(_lib.ref(pr), bt.n)
         ws = workspace(dev, "sum32", nbytes)
-        _lib.check(_lib.lib().msgb_sum_fwd_f32(_lib.ref(pr), _lib.ref(bs), _lib.ref(opts), ws.data_ptr(), nbytes,
-                                               out.data_ptr(), st), "msgb_sum_fwd_f32")
+        with self._kernel_span("msgb_sum_fwd_f32", cnt):
+            _lib.check(_lib.lib().msgb_sum_fwd_f32(_lib.ref(pr), _lib.ref(bs), _lib.ref(opts), ws.data_ptr(),
+                                                   nbytes, out.data_ptr(), st), "msgb_sum_fwd_f32")
         self._eval_counter = cnt
         return out
 
@@ -486,9 +549,10 @@ class MSGBSolver:
                             tiling=_lib.ref(tiling[0]) if tiling else None)
         nbytes = _lib.lib().msgb_sum_f32_workspace_size(_lib.ref(pr), bt.n)
         ws = workspace(dev, "sum32", nbytes)
-        _lib.check(_lib.lib().msgb_adj_gather_f32(_lib.ref(pr), _lib.ref(bs), _lib.ref(opts), ws.data_ptr(), nbytes,
-                                                  d.data_ptr(), torch.view_as_real(g).data_ptr(), st),
-                   "msgb_adj_gather_f32")
+        with self._kernel_span("msgb_adj_gather_f32", cnt):
+            _lib.check(_lib.lib().msgb_adj_gather_f32(_lib.ref(pr), _lib.ref(bs), _lib.ref(opts), ws.data_ptr(),
+                                                      nbytes, d.data_ptr(), torch.view_as_real(g).data_ptr(), st),
+                       "msgb_adj_gather_f32")
         self._eval_counter = cnt
         return g
 
@@ -521,6 +585,17 @@ class MSGBSolver:
         """Pressure at the sensors, shape (Nt, Ns) (msgb_solver.py:858-899)."""
         data, _ = self._forward_impl(p0, domain, sensors, ts, wpt, dpdt, want_params=False)
         return data
+
+    def forward_frozen(self, p0, domain: Domain, sensors, ts, wpt: MSWPT, selection: Selection):
+        """A_S p0: the forward with the beam selection S frozen, i.e. the
+        linear map whose exact transpose ``adjoint(..., selection=S)`` is.
+        The coefficients of p0 at S's indices drive S's beams."""
+        self._check_forward_args(p0, domain, ts, wpt, None)
+        x = as_device_f64(p0)
+        c = wpt.forward_device(x, self.input_type, scale=0.5, half_mask=True)
+        sel = Selection(selection.idx, c[selection.idx], selection.total_coeffs)
+        out = self.sum_forward(self.beams(sel, domain, wpt), domain, sensors, ts)
+        return out if _is_torch(p0) else out.cpu().numpy()
 
     def forward_with_params(self, p0, domain: Domain, sensors, ts, wpt: MSWPT, *, dpdt=None):
         """Sensor data and the beam parameters (p0s, M0s, x0s, omegas, a0s, modes)

@@ -205,6 +205,12 @@ typedef struct msgb_ode_opts {
     double rtol, atol;       /* DOPRI5: error norm RMS |e| / (atol + rtol max(|y0|, |y1|)) */
     double dt0;              /* DOPRI5 first step; <= 0 selects ts[1] - ts[0] */
     int64_t max_steps;       /* DOPRI5: accepted + rejected steps per beam */
+    int32_t only_flagged;    /* nonzero: integrate only beams whose out->status entry is
+                                nonzero (e.g. rejected surrogate predictions); the
+                                records of the others are left as they are */
+    int32_t dense_output;    /* DOPRI5 save times: 0 steps end on every save time (each
+                                step at most one save interval); 1 steps follow the error
+                                control and save times come from the continuous extension */
 } msgb_ode_opts;
 
 /* FP64 integration of coupled_rhs_absorption (gb/gb_solvers.py:787-867) for
@@ -242,6 +248,50 @@ int msgb_adj_gather_f32_traj(const msgb_problem *prob, const msgb_beam_set *beam
                              const msgb_trajectories *traj, const msgb_sum_opts *opts,
                              void *workspace, size_t workspace_bytes, const float *data, double *g,
                              msgb_stream_t stream);
+
+/* ---- trajectory surrogate: data path around the MLP -------------------- */
+/* No counterpart in the reference (it integrates every beam).  A BF16 MLP
+ * predicts each beam's state as a correction to the homogeneous closed form
+ * at c0 = c(x0); these entry points build its inputs and training targets
+ * from trajectories and turn predictions back into msgb_trajectories records.
+ * Rows are time-major: row q = kq * nb + (b - b_first). */
+typedef struct msgb_surrogate_io {
+    int64_t nb, b_first;       /* beams [b_first, b_first + nb) of the 2n */
+    int64_t nq_t;              /* time samples per beam */
+    const int32_t *t_index;    /* (nq_t) indices into ts, device; NULL: 0 .. nq_t - 1 */
+    int32_t ld;                /* row stride of X / Y in elements */
+} msgb_surrogate_io;
+
+/* Acceptance of predicted trajectories.  A beam is accepted when
+ * max_t |c(x)|p| / (c0 |p0|) - 1| <= residual_tol (status 3 otherwise) and
+ * w |p0| pos_err <= phase_tol (status 4 otherwise), pos_err being the
+ * surrogate's validated position error in metres. */
+typedef struct msgb_surrogate_accept {
+    double residual_tol;
+    double phase_tol;
+    double pos_err;
+} msgb_surrogate_accept;
+
+/* X (rows, ld) BF16 features: x0 / L, mode p0 / |p0|, log10 w - 3,
+ * log10 Im alpha + 3, (t - ts[0]) / (ts[nt-1] - ts[0]); 3d + 2 columns, the
+ * rest zero. */
+int msgb_surrogate_features(const msgb_problem *prob, const msgb_medium *med, const msgb_beam_set *beams,
+                            const msgb_surrogate_io *io, uint16_t *X, msgb_stream_t stream);
+/* Y (rows, ld) FP32 targets from rec64 (nt, nb, 2d + 2d^2 + 2) of the same
+ * chunk: (x - x_hom) / (c0 T), (p - p0) / |p0|, (M^-1 - M_hom^-1) |p0| / (c0 T)
+ * (upper triangle, real parts then imaginary parts), log(A / A_hom) (re, im):
+ * 6, 12 or 20 columns for d = 1, 2, 3. */
+int msgb_surrogate_targets(const msgb_problem *prob, const msgb_medium *med, const msgb_beam_set *beams,
+                           const msgb_surrogate_io *io, const double *rec64, float *Y,
+                           msgb_stream_t stream);
+/* Records from standardised predictions Y (every time, t_index NULL):
+ * y * stdv + mean per column, then the inverse of the target map.  Writes
+ * the records of beams [io->b_first, io->b_first + io->nb), which must lie in
+ * out's chunk, and their out->status entries (0 accepted, 3 or 4 rejected). */
+int msgb_surrogate_records(const msgb_problem *prob, const msgb_medium *med, const msgb_beam_set *beams,
+                           const msgb_surrogate_io *io, const float *Y, const float *mean,
+                           const float *stdv, const msgb_surrogate_accept *accept,
+                           const msgb_trajectories *out, msgb_stream_t stream);
 
 /* ---- tensor-core BF16 GEMM and MLP kernels (trajectory surrogate) ------ */
 
@@ -339,6 +389,27 @@ size_t msgb_topn_workspace_size(int64_t total, int64_t n);
 int msgb_topn(const double *keys, const double *coeffs, int64_t total, int64_t n,
               int64_t *idx, double *values, void *workspace, size_t workspace_bytes,
               msgb_stream_t stream);
+
+/* The other thresholds of threshold_coefficients (forward_solver_utils.py:
+ * 14-178, 181-230) over the same keys |c| and coefficients:
+ *   hard           |c| > val
+ *   percentile     |c| > jnp.percentile(|c|, val) ("linear")
+ *   hard_reassign  |c| >= val max|c|, values scaled by sqrt(sum|c|^2 / sum kept |c|^2)
+ *   bao_energy     |c| |centre of the coefficient's box|^d > val (needs plan)
+ *   perc_max_abs   |c| > val max|c|
+ * Writes the selected flat indices in ascending order to idx[0 .. *count),
+ * their (scaled) coefficients to values, and the count to *count (device). */
+enum {
+    MSGB_THR_HARD = 0,
+    MSGB_THR_PERCENTILE = 1,
+    MSGB_THR_HARD_REASSIGN = 2,
+    MSGB_THR_BAO_ENERGY = 3,
+    MSGB_THR_PERC_MAX_ABS = 4
+};
+size_t msgb_threshold_workspace_size(int64_t total);
+int msgb_threshold(int strategy, double val, const double *keys, const double *coeffs, int64_t total,
+                   const msgb_mswpt *plan, int64_t *idx, double *values, int64_t *count,
+                   void *workspace, size_t workspace_bytes, msgb_stream_t stream);
 
 /* ---- beam initialisation (forward_solver_utils.py:255-373) ------------- */
 

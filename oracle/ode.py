@@ -231,6 +231,9 @@ DP_A = ((),
 DP_B = (35 / 384, 0.0, 500 / 1113, 125 / 192, -2187 / 6784, 11 / 84, 0.0)
 DP_BHAT = (5179 / 57600, 0.0, 7571 / 16695, 393 / 640, -92097 / 339200, 187 / 2100, 1 / 40)
 DP_E = tuple(b - bh for b, bh in zip(DP_B, DP_BHAT))
+# Continuous-extension weights (Shampine 1986; Hairer, Norsett & Wanner's dopri5).
+DP_D = (-12715105075 / 11282082432, 0.0, 87487479700 / 32700410799, -10690763975 / 1880347072,
+        701980252875 / 199316789632, -1453857185 / 822651844, 69997945 / 29380423)
 
 
 def error_norm(e, y0, y1, d, rtol, atol):
@@ -245,62 +248,89 @@ def error_norm(e, y0, y1, d, rtol, atol):
     return float(np.sqrt(np.mean(r * r)))
 
 
-def dopri5(x0, p0, M0, a0, mode, ts, speed, lam=0.0, rtol=1e-7, atol=1e-9, max_steps=4096, dt0=None):
+def dense_state(y, y5, ks, h, theta):
+    """Dormand-Prince continuous extension (Shampine's 4th-order interpolant,
+    the form of Hairer, Norsett & Wanner's dopri5 contd5) at t + theta h."""
+    r2 = y5 - y
+    r3 = h * ks[0] - r2
+    r4 = r2 - h * ks[6] - r3
+    r5 = h * sum(c * kk for c, kk in zip(DP_D, ks) if c != 0.0)
+    return y + theta * (r2 + (1.0 - theta) * (r3 + theta * (r4 + (1.0 - theta) * r5)))
+
+
+def dopri5(x0, p0, M0, a0, mode, ts, speed, lam=0.0, rtol=1e-7, atol=1e-9, max_steps=4096, dt0=None,
+           dense=False):
     """Adaptive Dormand-Prince 5(4) of ``rhs`` with the state saved at every ts.
 
     Step control (the GPU integrator's, step for step): error norm as
     ``error_norm``; accept when it is <= 1; next step h * clip(0.9 err^(-1/5),
-    0.2, 10) (at most 1 after a rejection); steps are shortened to land on each
-    save time, and after such a landing the previous proposal is kept if larger.
+    0.2, 10) (at most 1 after a rejection, and for the step that follows an
+    accepted step that came right after a rejection).  Save times: by default
+    a step that would pass the next save time is shortened to end on it (the
+    proposal it replaced is kept for the next step); with ``dense`` steps
+    follow the error control alone (the last one shortened to end at ts[-1])
+    and save times inside a step are read from the continuous extension
+    (``dense_state``), as diffrax's SaveAt(ts) reads its solver's interpolant.
     ``max_steps`` counts accepted and rejected steps over the whole solve, as
     diffrax does (gb/gb_solvers.py:756-783 builds that solve: Tsit5,
     PIDController(rtol, atol), SaveAt(ts), dt0 = ts[1] - ts[0]).
     Returns (xt, pt, Mt, At, status, steps); status 0 ok, 1 non-finite,
-    2 max_steps reached.
+    2 max_steps reached (later save times then hold the last state).
     """
     d = len(x0)
     y = _pack_state(x0, p0, M0, a0)
     ts = np.asarray(ts, float)
+    nt = ts.size
     f = lambda v: rhs(0.0, v, mode, speed, d, lam)
-    h = float(dt0) if dt0 is not None else (ts[1] - ts[0] if ts.size > 1 else 0.0)
+    h = float(dt0) if dt0 is not None else (ts[1] - ts[0] if nt > 1 else 0.0)
     out = [y.copy()]
     steps, status = 0, 0
     k1 = f(y)
     t = ts[0]
-    for k in range(1, ts.size):
-        t_end = ts[k]
-        while status == 0 and t < t_end:
-            if steps >= max_steps:
-                status = 2
-                break
-            hh, clipped = h, False
-            if t + hh >= t_end:
-                hh, clipped = t_end - t, True
-            ks = [k1]
-            for s in range(1, 7):
-                acc = np.zeros_like(y)
-                for j, a in enumerate(DP_A[s]):
-                    if a != 0.0:
-                        acc = acc + a * ks[j]
-                ks.append(f(y + hh * acc))
-            y5 = y + hh * sum(b * kk for b, kk in zip(DP_B, ks) if b != 0.0)
-            # stage 7 is evaluated at y + hh * sum(a7j k_j), which is y5 up to rounding
-            e = hh * sum(c * kk for c, kk in zip(DP_E, ks))
-            err = error_norm(e, y, y5, d, rtol, atol)
-            steps += 1
-            if not np.isfinite(err):
-                h = 0.2 * hh
-                continue
-            fac = 10.0 if err == 0.0 else min(10.0, max(0.2, 0.9 * err ** -0.2))
-            if err <= 1.0:
-                t = t_end if clipped else t + hh
-                y = y5
-                k1 = ks[6]
-                hn = hh * fac
-                h = max(hn, h) if clipped else hn
-            else:
-                h = hh * min(1.0, fac)
-        if status == 0 and not np.all(np.isfinite(y)):
-            status = 1
+    k = 1
+    rejected = False
+    while k < nt and status == 0:
+        if steps >= max_steps:
+            status = 2
+            break
+        target = ts[-1] if dense else ts[k]
+        hh, last = h, False
+        if t + hh >= target:
+            hh, last = target - t, True
+        ks = [k1]
+        for s in range(1, 7):
+            acc = np.zeros_like(y)
+            for j, a in enumerate(DP_A[s]):
+                if a != 0.0:
+                    acc = acc + a * ks[j]
+            ks.append(f(y + hh * acc))
+        y5 = y + hh * sum(b * kk for b, kk in zip(DP_B, ks) if b != 0.0)
+        # stage 7 is evaluated at y + hh * sum(a7j k_j), which is y5 up to rounding
+        e = hh * sum(c * kk for c, kk in zip(DP_E, ks))
+        err = error_norm(e, y, y5, d, rtol, atol)
+        steps += 1
+        if not np.isfinite(err):
+            h = 0.2 * hh
+            rejected = True
+            continue
+        fac = 10.0 if err == 0.0 else min(10.0, max(0.2, 0.9 * err ** -0.2))
+        if err <= 1.0:
+            if rejected:
+                fac = min(fac, 1.0)
+            rejected = False
+            t_new = target if last else t + hh
+            while k < nt and ts[k] <= t_new:
+                out.append(y5.copy() if ts[k] == t_new else dense_state(y, y5, ks, hh, (ts[k] - t) / hh))
+                k += 1
+            t = t_new
+            y = y5
+            k1 = ks[6]
+            h = max(hh * fac, h) if (last and not dense) else hh * fac
+            if not np.all(np.isfinite(y)):
+                status = 1
+        else:
+            h = hh * min(1.0, fac)
+            rejected = True
+    while len(out) < nt:
         out.append(y.copy())
     return _unpack_states(out, d) + (status, steps)

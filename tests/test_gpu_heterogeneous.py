@@ -5,9 +5,10 @@ Oracles: the oracle's own RK4 and Dormand-Prince 5(4) of coupled_rhs_absorption
 implementation parity; SciPy DOP853 at rtol = atol = 1e-12 (the reference
 test's own oracle, tests/test_gb.py:759-849) for the methods' accuracy.
 Tolerances: GPU RK4 equal to the oracle RK4 to round-off and the adaptive
-integrator to 1e-9; against DOP853 rays within 1e-8, M within 1e-4 at the
+integrator to 1e-9 (1e-5 / 1e-4 with the continuous extension, where step
+decisions can flip); against DOP853 rays within 1e-8, M within 1e-4 at the
 default rtol 1e-7 (1e-6 at rtol 1e-10), fixed-step M converging at second
-order; the FP64 forward within 1e-6 rel-L2 of the oracle sum over oracle
+order; the FP64 forward within 1e-7 rel-L2 of the oracle sum over oracle
 trajectories; FP32 within 1e-3 of FP64; the transpose's dot test at 1e-10.
 """
 
@@ -65,10 +66,11 @@ def _rk4_states(ndim, x0, p0, alpha, ts, medium, L, periodic=None, substeps=1, o
     return rec.cpu().numpy()
 
 
-def _dopri(rtol=1e-7, atol=1e-9, max_steps=4096):
+def _dopri(rtol=1e-7, atol=1e-9, max_steps=4096, dense=False):
     from beamax_b200 import _lib
 
-    return _lib.OdeOpts(method=1, substeps=1, rtol=rtol, atol=atol, dt0=0.0, max_steps=max_steps)
+    return _lib.OdeOpts(method=1, substeps=1, rtol=rtol, atol=atol, dt0=0.0, max_steps=max_steps,
+                        dense_output=int(dense))
 
 
 def _grid_medium(interp):
@@ -163,29 +165,34 @@ def test_rk4_converges_to_dop853_in_smooth_bspline_medium():
 
 def test_dopri5_matches_oracle_dopri5_in_sharp_bspline_medium():
     """Adaptive integrator == the oracle's Dormand-Prince 5(4) with the same
-    step control (default tolerances) to 1e-9."""
+    step control (default tolerances).  Steps ending on the save times: equal
+    to 1e-9.  Continuous extension: steps are longer and a round-off flip of
+    one accept/reject decision changes the step sequence, after which the
+    solutions agree to the tolerance: rays 1e-5, M and A 1e-4."""
     N, dx = (64, 64), (1e-4, 1e-4)
     c, interp = _random_medium(N, dx, 0.1, 6.0, 3)
     n, x0, p0, alpha = _beams3()
     ts = np.arange(0, 80) * 2e-8
     speed = oo.GridSpeed(c, dx, method="bspline3", boundary="clamp")
-    rec = _rk4_states(2, x0, p0, alpha, ts, _grid_medium(interp), (64e-4, 64e-4), ode=_dopri())
-    for b in range(2 * n):
-        j, mode = b % n, (1.0 if b < n else -1.0)
-        ox, op, oM, oA, st, steps = oo.dopri5(x0[j], p0[j], np.diag(alpha[j]), 1.0, mode, ts, speed)
-        assert st == 0
-        gx, gp, gM, gA = _unpack(rec[:, b], 2)
-        assert np.max(np.abs(gx - ox)) <= 1e-9 * np.max(np.abs(ox))
-        assert np.max(np.abs(gp - op)) <= 1e-9 * np.max(np.abs(op))
-        assert np.max(np.abs(gM - oM)) <= 1e-9 * np.max(np.abs(oM))
-        assert np.max(np.abs(gA - oA)) <= 1e-9 * np.max(np.abs(oA))
+    med = _grid_medium(interp)
+    for dense, tol, tol_m in ((False, 1e-9, 1e-9), (True, 1e-5, 1e-4)):
+        rec = _rk4_states(2, x0, p0, alpha, ts, med, (64e-4, 64e-4), ode=_dopri(dense=dense))
+        for b in range(2 * n):
+            j, mode = b % n, (1.0 if b < n else -1.0)
+            ox, op, oM, oA, st, steps = oo.dopri5(x0[j], p0[j], np.diag(alpha[j]), 1.0, mode, ts, speed, dense=dense)
+            assert st == 0
+            gx, gp, gM, gA = _unpack(rec[:, b], 2)
+            assert np.max(np.abs(gx - ox)) <= tol * np.max(np.abs(ox))
+            assert np.max(np.abs(gp - op)) <= tol * np.max(np.abs(op))
+            assert np.max(np.abs(gM - oM)) <= tol_m * np.max(np.abs(oM))
+            assert np.max(np.abs(gA - oA)) <= tol_m * np.max(np.abs(oA))
 
 
 def test_dopri5_accuracy_against_dop853():
-    """The adaptive integrator's global error against DOP853 at 1e-12: at the
-    reference's default rtol 1e-7 / atol 1e-9 rays within 1e-8 and M within
-    1e-4; at rtol 1e-10 / atol 1e-12, M within 1e-6 (it converges with the
-    tolerance, unlike fixed steps)."""
+    """The adaptive integrator's global error against DOP853 at 1e-12 (steps
+    ending on the save times): at the reference's default rtol 1e-7 / atol
+    1e-9 rays within 1e-8 and M within 1e-4; at rtol 1e-10 / atol 1e-12, M
+    within 1e-6 (it converges with the tolerance, unlike fixed steps)."""
     N, dx = (64, 64), (1e-4, 1e-4)
     c, interp = _random_medium(N, dx, 0.1, 16.0, 5)
     n, x0, p0, alpha = _beams3(2)
@@ -285,9 +292,7 @@ def _het_case(seed=0, N=(64, 64), thr=24):
 def test_heterogeneous_forward_fp64_matches_oracle():
     """GPU FP64 forward (adaptive ODE + dense sum) == the oracle's Dormand-Prince
     trajectories summed with the oracle's summation (gb/core.py:194-329), to
-    1e-6 rel-L2: an accept/reject decision taken at an error norm within
-    round-off of 1 can go either way, after which the two solutions differ by
-    up to the local tolerance (rtol 1e-7), and the phase multiplies that by w."""
+    1e-7 rel-L2 (the phase multiplies position round-off by w |p|)."""
     import beamax_b200 as bb
 
     _dev()
@@ -304,7 +309,7 @@ def test_heterogeneous_forward_fp64_matches_oracle():
             xt, pt, Mt, At, st, _ = oo.dopri5(x0[j], p0s[j], np.diag(al[j]), a0[j], mode, ts, speed)
             assert st == 0
             ref += oo.beam_field(xt, pt, Mt, At, w[j], sens.positions, dom.grid_size, dom.periodic)
-    assert om.rel_l2(ref, out) < 1e-6
+    assert om.rel_l2(ref, out) < 1e-7
 
 
 def test_heterogeneous_fp32_and_adjoint_dot_test():
