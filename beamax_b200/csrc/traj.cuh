@@ -75,6 +75,9 @@ __device__ void speed_eval(const MediumArgs &m, const double *x, double &c, doub
         }
         for (int k = 0; k < taps; ++k) idx[a][k] = map_index(i0 + off0 + k, m.n[a], m.boundary);
     }
+    // Separable reduction, last axis first: the tensor-product weights factor,
+    // so the value, gradient and Hessian need 3 sums per line of the last
+    // axis instead of D^2 products per grid corner.
     double cc = 0.0, gg[D], hh[D][D];
 #pragma unroll
     for (int i = 0; i < D; ++i) {
@@ -82,43 +85,61 @@ __device__ void speed_eval(const MediumArgs &m, const double *x, double &c, doub
 #pragma unroll
         for (int k = 0; k < D; ++k) hh[i][k] = 0.0;
     }
-    const int ncorner = D == 1 ? taps : (D == 2 ? taps * taps : taps * taps * taps);
-    for (int corner = 0; corner < ncorner; ++corner) {
-        int loc[D];
-        int rem = corner;
-        int64_t flat = 0;
-#pragma unroll
-        for (int a = D - 1; a >= 0; --a) {
-            loc[a] = rem % taps;
-            rem /= taps;
+    if (D == 1) {
+        for (int k = 0; k < taps; ++k) {
+            const double v = __ldg(m.coeffs + idx[0][k]);
+            cc = fma(w[0][k], v, cc);
+            gg[0] = fma(d1[0][k], v, gg[0]);
+            hh[0][0] = fma(d2[0][k], v, hh[0][0]);
         }
-#pragma unroll
-        for (int a = 0; a < D; ++a) flat = flat * m.n[a] + idx[a][loc[a]];
-        const double v = __ldg(m.coeffs + flat);
-        double wall = 1.0;
-#pragma unroll
-        for (int a = 0; a < D; ++a) wall *= w[a][loc[a]];
-        cc = fma(wall, v, cc);
-#pragma unroll
-        for (int a = 0; a < D; ++a) {
-            double ga = d1[a][loc[a]];
-            double ha = d2[a][loc[a]];
-#pragma unroll
-            for (int o = 0; o < D; ++o)
-                if (o != a) {
-                    ga *= w[o][loc[o]];
-                    ha *= w[o][loc[o]];
-                }
-            gg[a] = fma(ga, v, gg[a]);
-            hh[a][a] = fma(ha, v, hh[a][a]);
-#pragma unroll
-            for (int b = a + 1; b < D; ++b) {
-                double hab = d1[a][loc[a]] * d1[b][loc[b]];
-#pragma unroll
-                for (int o = 0; o < D; ++o)
-                    if (o != a && o != b) hab *= w[o][loc[o]];
-                hh[a][b] = fma(hab, v, hh[a][b]);
+    } else if (D == 2) {
+        const int L = D - 1;  // last axis
+        for (int i = 0; i < taps; ++i) {
+            const double *row = m.coeffs + (int64_t)idx[0][i] * m.n[L];
+            double rw = 0.0, rd = 0.0, rdd = 0.0;
+            for (int k = 0; k < taps; ++k) {
+                const double v = __ldg(row + idx[L][k]);
+                rw = fma(w[L][k], v, rw);
+                rd = fma(d1[L][k], v, rd);
+                rdd = fma(d2[L][k], v, rdd);
             }
+            cc = fma(w[0][i], rw, cc);
+            gg[0] = fma(d1[0][i], rw, gg[0]);
+            gg[L] = fma(w[0][i], rd, gg[L]);
+            hh[0][0] = fma(d2[0][i], rw, hh[0][0]);
+            hh[0][L] = fma(d1[0][i], rd, hh[0][L]);
+            hh[L][L] = fma(w[0][i], rdd, hh[L][L]);
+        }
+    } else {
+        const int Y = 1 % D, Z = 2 % D;
+        for (int i = 0; i < taps; ++i) {
+            double tw = 0.0, ty = 0.0, tyy = 0.0, tz = 0.0, tyz = 0.0, tzz = 0.0;
+            for (int j = 0; j < taps; ++j) {
+                const double *line = m.coeffs + ((int64_t)idx[0][i] * m.n[Y] + idx[Y][j]) * m.n[Z];
+                double sw = 0.0, sd = 0.0, sdd = 0.0;
+                for (int k = 0; k < taps; ++k) {
+                    const double v = __ldg(line + idx[Z][k]);
+                    sw = fma(w[Z][k], v, sw);
+                    sd = fma(d1[Z][k], v, sd);
+                    sdd = fma(d2[Z][k], v, sdd);
+                }
+                tw = fma(w[Y][j], sw, tw);
+                ty = fma(d1[Y][j], sw, ty);
+                tyy = fma(d2[Y][j], sw, tyy);
+                tz = fma(w[Y][j], sd, tz);
+                tyz = fma(d1[Y][j], sd, tyz);
+                tzz = fma(w[Y][j], sdd, tzz);
+            }
+            cc = fma(w[0][i], tw, cc);
+            gg[0] = fma(d1[0][i], tw, gg[0]);
+            gg[Y] = fma(w[0][i], ty, gg[Y]);
+            gg[Z] = fma(w[0][i], tz, gg[Z]);
+            hh[0][0] = fma(d2[0][i], tw, hh[0][0]);
+            hh[0][Y] = fma(d1[0][i], ty, hh[0][Y]);
+            hh[0][Z] = fma(d1[0][i], tz, hh[0][Z]);
+            hh[Y][Y] = fma(w[0][i], tyy, hh[Y][Y]);
+            hh[Y][Z] = fma(w[0][i], tyz, hh[Y][Z]);
+            hh[Z][Z] = fma(w[0][i], tzz, hh[Z][Z]);
         }
     }
     c = cc;

@@ -104,12 +104,16 @@ class MSGBSolver:
       surrogate: a fitted ``beamax_b200.surrogate.TrajectorySurrogate`` for the
         medium and time grid; heterogeneous beams are predicted by it and the
         ones it does not accept are integrated.
+      keep_trajectories: in heterogeneous media, keep the last forward's
+        trajectory records on the device (when they fit in trajectory_memory)
+        so that an adjoint with the same selection, domain and time grid does
+        not integrate the beams again.
     """
 
     def __init__(self, thr, thr_strat: str, batch_size: int, input_type: str, ode_solver, sum_method: str,
                  tr_ode_solver=None, sharding=None, ode_config=None, adjoint_relative_guard: float = 5e-2,
                  *, precision: str = "fp64", cutoff: float = 16.0, rk4_substeps: int = 1,
-                 trajectory_memory: int = 16 << 30, surrogate=None):
+                 trajectory_memory: int = 40 << 30, surrogate=None, keep_trajectories: bool = True):
         valid_thresholds = {"hard", "top_n", "percentile", "hard_reassign", "bao_energy", "perc_max_abs"}
         if thr_strat not in valid_thresholds:
             raise ValueError(f"thr_strat must be one of {', '.join(sorted(valid_thresholds))}; got {thr_strat!r}.")
@@ -168,6 +172,9 @@ class MSGBSolver:
         self.rk4_substeps = max(int(rk4_substeps), ode_config.substeps)
         self.trajectory_memory = int(trajectory_memory)
         self.surrogate = surrogate
+        self.keep_trajectories = bool(keep_trajectories)
+        self._traj_cache = None
+        self._traj_owner = None
         # When set to a list, every FP32 summation entry point call appends
         # (name, start event, end event, evaluation counter) recorded on the
         # launching stream around the call.
@@ -364,8 +371,9 @@ class MSGBSolver:
                             dt0=float(cfg.dt0) if cfg.dt0 is not None else 0.0, max_steps=int(cfg.max_steps),
                             dense_output=int(bool(cfg.dense_output)))
 
-    def _trajectories(self, pr, med, bs, b_first, nb, fp64, per, n_tt, dev, st, status):
-        buf = workspace(dev, "traj", per * nb + 4096)
+    def _trajectories(self, pr, med, bs, b_first, nb, fp64, per, n_tt, dev, st, status, buf=None):
+        if buf is None:
+            buf = workspace(dev, "traj", per * nb + 4096)
         base = buf.data_ptr()
         d = pr.ndim
         S = d * (d + 1) // 2
@@ -380,8 +388,9 @@ class MSGBSolver:
             acc = (status[b_first:b_first + nb] == 0).sum()
             self._accepted = acc if self._accepted is None else self._accepted + acc
             opts.only_flagged = 1
-        _lib.check(_lib.lib().msgb_ode_trajectories(_lib.ref(pr), _lib.ref(med), _lib.ref(bs), _lib.ref(opts),
-                                                    _lib.ref(tr), st), "msgb_ode_trajectories")
+        with self._kernel_span("msgb_ode_trajectories", None):
+            _lib.check(_lib.lib().msgb_ode_trajectories(_lib.ref(pr), _lib.ref(med), _lib.ref(bs), _lib.ref(opts),
+                                                        _lib.ref(tr), st), "msgb_ode_trajectories")
         return tr, buf
 
     def _begin_trajectories(self, domain, ts):
@@ -429,13 +438,18 @@ class MSGBSolver:
         chunks, per, n_tt = self._chunks(domain, pr.nt, 2 * bt.n, fp64)
         status = torch.zeros(2 * bt.n, dtype=torch.int32, device=dev)
         self._begin_trajectories(domain, ts)
+        self._traj_cache = None
+        keep_buf = None
+        if self.keep_trajectories and self._traj_owner is not None and len(chunks) == 1:
+            keep_buf = torch.empty(per * chunks[0][1] + 4096, dtype=torch.uint8, device=dev)
         if fp64:
             out = torch.zeros((pr.nt, pr.ns), dtype=torch.float64, device=dev)
             for b_first, nb in chunks:
-                tr, _ = self._trajectories(pr, med, bs, b_first, nb, True, per, n_tt, dev, st, status)
+                tr, buf = self._trajectories(pr, med, bs, b_first, nb, True, per, n_tt, dev, st, status, keep_buf)
                 _lib.check(_lib.lib().msgb_sum_fwd_f64_traj(_lib.ref(pr), _lib.ref(bs), _lib.ref(tr), out.data_ptr(),
                                                             st), "msgb_sum_fwd_f64_traj")
             self._check_status(status)
+            self._remember_trajectories(keep_buf, tr, domain, ts, pr.nt)
             return out
         out = torch.empty((pr.nt, pr.ns), dtype=torch.float32, device=dev)
         cnt = torch.zeros(1, dtype=torch.int64, device=dev)
@@ -445,15 +459,31 @@ class MSGBSolver:
         nbytes = _lib.lib().msgb_sum_f32_traj_workspace_size(_lib.ref(pr), 2 * bt.n)
         ws = workspace(dev, "sum32traj", nbytes)
         for i, (b_first, nb) in enumerate(chunks):
-            tr, _ = self._trajectories(pr, med, bs, b_first, nb, False, per, n_tt, dev, st, status)
-            _lib.check(_lib.lib().msgb_sum_fwd_f32_traj(_lib.ref(pr), _lib.ref(bs), _lib.ref(tr), _lib.ref(opts),
-                                                        int(i == 0), int(i == len(chunks) - 1), ws.data_ptr(), nbytes,
-                                                        out.data_ptr(), st), "msgb_sum_fwd_f32_traj")
+            tr, buf = self._trajectories(pr, med, bs, b_first, nb, False, per, n_tt, dev, st, status, keep_buf)
+            with self._kernel_span("msgb_sum_fwd_f32_traj", cnt):
+                _lib.check(_lib.lib().msgb_sum_fwd_f32_traj(_lib.ref(pr), _lib.ref(bs), _lib.ref(tr), _lib.ref(opts),
+                                                            int(i == 0), int(i == len(chunks) - 1), ws.data_ptr(),
+                                                            nbytes, out.data_ptr(), st), "msgb_sum_fwd_f32_traj")
         self._eval_counter = cnt
         self._check_status(status)
+        self._remember_trajectories(keep_buf, tr, domain, ts, pr.nt)
         return out
 
-    def _gather_adjoint_het(self, bt: BeamTensors, domain: Domain, sensors, ts, data):
+    def _remember_trajectories(self, buf, tr, domain, ts, nt):
+        if buf is None:
+            self._traj_cache = None
+            return
+        self._traj_cache = {"selection": self._traj_owner, "domain": domain, "ts": ts, "nt": nt,
+                            "precision": self.precision, "tr": tr, "buf": buf}
+
+    def _cached_trajectories(self, selection, domain, ts):
+        c = self._traj_cache
+        if (c is not None and c["selection"] is selection and c["domain"] is domain and c["ts"] is ts
+                and c["precision"] == self.precision):
+            return c
+        return None
+
+    def _gather_adjoint_het(self, bt: BeamTensors, domain: Domain, sensors, ts, data, cached=None):
         import torch
 
         dev = bt.x0.device
@@ -479,16 +509,22 @@ class MSGBSolver:
         ws = None if fp64 else workspace(dev, "sum32traj", nbytes)
         status = torch.zeros(2 * n, dtype=torch.int32, device=dev)
         self._begin_trajectories(domain, ts)
+        if cached is not None:
+            chunks = [(0, 2 * n)]
         for b_first, nb in chunks:
-            tr, _ = self._trajectories(pr, med, bs, b_first, nb, fp64, per, n_tt, dev, st, status)
+            if cached is not None:
+                tr = cached["tr"]  # the forward's records for these beams, in this order
+            else:
+                tr, _ = self._trajectories(pr, med, bs, b_first, nb, fp64, per, n_tt, dev, st, status)
             gp = torch.view_as_real(g_all[b_first:b_first + nb]).data_ptr()
             if fp64:
                 _lib.check(_lib.lib().msgb_adj_gather_f64_traj(_lib.ref(pr), _lib.ref(bs), _lib.ref(tr), d.data_ptr(),
                                                                gp, st), "msgb_adj_gather_f64_traj")
             else:
-                _lib.check(_lib.lib().msgb_adj_gather_f32_traj(_lib.ref(pr), _lib.ref(bs), _lib.ref(tr), _lib.ref(opts),
-                                                               ws.data_ptr(), nbytes, d.data_ptr(), gp, st),
-                           "msgb_adj_gather_f32_traj")
+                with self._kernel_span("msgb_adj_gather_f32_traj", cnt):
+                    _lib.check(_lib.lib().msgb_adj_gather_f32_traj(_lib.ref(pr), _lib.ref(bs), _lib.ref(tr),
+                                                                   _lib.ref(opts), ws.data_ptr(), nbytes,
+                                                                   d.data_ptr(), gp, st), "msgb_adj_gather_f32_traj")
         self._eval_counter = cnt
         self._check_status(status)
         return g_all[:n] + g_all[n:]
@@ -522,12 +558,12 @@ class MSGBSolver:
         self._eval_counter = cnt
         return out
 
-    def gather_adjoint(self, bt: BeamTensors, domain: Domain, sensors, ts, data):
+    def gather_adjoint(self, bt: BeamTensors, domain: Domain, sensors, ts, data, _cached=None):
         """Per selected coefficient g_j = sum 2 d conj(K_j) over both modes: (n,) complex128."""
         import torch
 
         if self.heterogeneous(domain):
-            return self._gather_adjoint_het(bt, domain, sensors, ts, data)
+            return self._gather_adjoint_het(bt, domain, sensors, ts, data, _cached)
 
         dev = bt.x0.device
         pr, keep = self._problem(domain, sensors, ts, dev)
@@ -608,7 +644,11 @@ class MSGBSolver:
         self._sensor_positions(sensors)
         sel = self.select(p0, domain, wpt, dpdt)
         bt = self.beams(sel, domain, wpt)
-        out = self.sum_forward(bt, domain, sensors, ts)
+        self._traj_owner = sel
+        try:
+            out = self.sum_forward(bt, domain, sensors, ts)
+        finally:
+            self._traj_owner = None
         self.last_selection = sel
         result = out if _is_torch(p0) else out.cpu().numpy()
         if not want_params:
@@ -671,10 +711,14 @@ class MSGBSolver:
         # Gather in flat-index order: neighbouring coefficients (same box,
         # adjacent packet positions) have overlapping footprints, so the
         # per-beam warps of a CTA reuse the same data tiles from L1.
-        order = torch_argsort(selection.idx)
-        sel_sorted = Selection(selection.idx[order], selection.values[order], selection.total_coeffs)
+        cached = self._cached_trajectories(selection, domain, ts) if self.heterogeneous(domain) else None
+        if cached is not None:
+            sel_sorted = selection  # the order of the kept trajectory records
+        else:
+            order = torch_argsort(selection.idx)
+            sel_sorted = Selection(selection.idx[order], selection.values[order], selection.total_coeffs)
         bt = self.beams(sel_sorted, domain, wpt)
-        g = self.gather_adjoint(bt, domain, sensors, ts, data)
+        g = self.gather_adjoint(bt, domain, sensors, ts, data, cached)
         img = self.coefficient_adjoint(sel_sorted, g, wpt)
         return img if _is_torch(data) else img.cpu().numpy()
 

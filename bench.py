@@ -19,6 +19,12 @@ per second of forward + adjoint (2 * 2n * Nt * Ns per step / step time).
 ``--impl reference`` times the CPU restatement of the reference algorithm
 (C/OpenMP FP64, dense, all host threads) on a bounded beam sample and
 reports the same metric.
+
+``--workload het512`` / ``c3`` measure the heterogeneous path instead
+(seeded random sound speed, adaptive FP64 beam ODE, trajectory summation):
+het512 is config 2's geometry in a 20-cell-correlation medium, c3 the 1024^2,
+dx 5e-5, 40-cell-correlation configuration with the valid 4-level tiling and
+thr 262,144 (its dense FP64 comparison takes minutes).
 """
 
 from __future__ import annotations
@@ -91,7 +97,52 @@ def config2(seed=0, thr=65536):
     ts = dom.generate_time_domain()
     p0 = make_p0(N, (4, 8, 16, 32), 64, 8, 20.0, seed)
     return dict(name=f"config2: 2D 512^2 homogeneous, 4 levels (4,8,16,32), four-sided sensor, thr={thr}",
-                domain=dom, wpt=wpt, sensors=sensors, ts=ts, p0=p0, thr=thr)
+                domain=dom, wpt=wpt, sensors=sensors, ts=ts, p0=p0, thr=thr, hetero=False)
+
+
+def random_speed(N, dx, contrast, corr_cells, seed):
+    """c = 1500 (1 + contrast g), g a seeded Gaussian random field with the
+    given correlation length (cells), scaled to max |g| = 1 and clipped to
+    [-1, 1]; cubic B-spline interpolant with clamped boundaries."""
+    from scipy import ndimage
+
+    from beamax_b200.utils.interp import make_c_function_from_grid
+
+    rng = np.random.default_rng(seed)
+    g = ndimage.gaussian_filter(rng.standard_normal(N), corr_cells, mode="wrap")
+    g = np.clip(g / np.max(np.abs(g)), -1.0, 1.0)
+    return make_c_function_from_grid(1500.0 * (1.0 + contrast * g), dx, method="bspline3", boundary="clamp")
+
+
+def heterogeneous(N, dx, corr_cells, n_packets, thr, seed, name):
+    import beamax_b200 as bb
+
+    c = random_speed(N, dx, 0.08, corr_cells, seed + 17)
+    dom = bb.Domain(N=N, dx=dx, periodic=(False, False), cfl=0.3, c=c)
+    dec = bb.DyadicDecomposition(4, N, (4, 8, 16, 32), (1, 1))
+    wpt = bb.MSWPT(dec, 2, "rectangular_mirror")
+    mask = np.zeros(N)
+    mask[0, :] = mask[-1, :] = mask[:, 0] = mask[:, -1] = 1
+    sensors = bb.Sensor(dom, binary_mask=mask)
+    ts = dom.generate_time_domain()
+    p0 = make_p0(N, (4, 8, 16, 32), n_packets, 8, 20.0 * N[0] / 512, seed)
+    return dict(name=name, domain=dom, wpt=wpt, sensors=sensors, ts=ts, p0=p0, thr=thr, hetero=True)
+
+
+def het512(seed=0, thr=65536):
+    return heterogeneous((512, 512), (1e-4, 1e-4), 20.0, 64, thr, seed,
+                         f"het512: 2D 512^2, c = 1500 (1 + 0.08 g), 20-cell correlation, 4 levels (4,8,16,32), "
+                         f"four-sided sensor, thr={thr}, adaptive ODE")
+
+
+def config3(seed=0, thr=262144):
+    return heterogeneous((1024, 1024), (5e-5, 5e-5), 40.0, 256, thr, seed,
+                         f"config3: 2D 1024^2, dx 5e-5, c = 1500 (1 + 0.08 g), 40-cell correlation, 4 levels "
+                         f"(4,8,16,32), four-sided sensor, thr={thr}, adaptive ODE")
+
+
+WORKLOADS = {"c2": config2, "het512": het512, "c3": config3}
+DEFAULT_THR = {"c2": 65536, "het512": 65536, "c3": 262144}
 
 
 # ---------------------------------------------------------------- clocks
@@ -154,11 +205,11 @@ def run_ours(args, rank, world, device):
     from beamax_b200.solvers.msgb_solver import Selection
 
     torch.cuda.set_device(device)
-    W = config2(seed=1234 + rank, thr=args.thr)
+    W = WORKLOADS[args.workload](seed=1234 + rank, thr=args.thr)
     dom, wpt, sens, ts, p0 = W["domain"], W["wpt"], W["sensors"], W["ts"], W["p0"]
-    hom = bb.gb.gb_solvers.solve_hom_diag
-    s32 = bb.MSGBSolver(W["thr"], "top_n", 128, "spatial", hom, "scan_real", precision="fp32", cutoff=args.cutoff)
-    s64 = bb.MSGBSolver(W["thr"], "top_n", 128, "spatial", hom, "scan_real", precision="fp64")
+    ode = bb.gb.gb_solvers.solve_ODE_base if W["hetero"] else bb.gb.gb_solvers.solve_hom_diag
+    s32 = bb.MSGBSolver(W["thr"], "top_n", 128, "spatial", ode, "scan_real", precision="fp32", cutoff=args.cutoff)
+    s64 = bb.MSGBSolver(W["thr"], "top_n", 128, "spatial", ode, "scan_real", precision="fp64")
     p0_d = torch.from_numpy(p0).to(device)
     nt, ns = ts.size, sens.positions.shape[0]
     n = W["thr"]
@@ -201,12 +252,18 @@ def run_ours(args, rank, world, device):
     spans = s32.kernel_timer
     s32.kernel_timer = None
 
-    def span_stats(name):
-        sel = [(a.elapsed_time(b) / 1e3, int(c.item())) for nm, a, b, c in spans if nm == name]
-        return float(np.mean([t for t, _ in sel])), int(np.mean([e for _, e in sel]))
+    def span_time(name):
+        """Device time per step of every call of one entry point (all chunks)."""
+        return sum(a.elapsed_time(b) / 1e3 for nm, a, b, c in spans if nm == name) / args.steps
 
-    t_fwd_kernel, fwd_evals = span_stats("msgb_sum_fwd_f32")
-    t_adj_kernel, adj_evals = span_stats("msgb_adj_gather_f32")
+    def span_evals(name):
+        cs = [c for nm, a, b, c in spans if nm == name]
+        return int(cs[-1].item()) if cs else 0  # one counter per call, summed over its chunks
+
+    suffix = "_traj" if W["hetero"] else ""
+    t_fwd_kernel, fwd_evals = span_time("msgb_sum_fwd_f32" + suffix), span_evals("msgb_sum_fwd_f32" + suffix)
+    t_adj_kernel, adj_evals = span_time("msgb_adj_gather_f32" + suffix), span_evals("msgb_adj_gather_f32" + suffix)
+    t_ode = span_time("msgb_ode_trajectories")
     total = float(np.sum(times))
     if world > 1:
         t = torch.tensor([total], dtype=torch.float64, device=device)
@@ -231,6 +288,9 @@ def run_ours(args, rank, world, device):
     e2e_t = float(np.mean(e2e))
 
     result = {"rank": rank, "t_step": total / args.steps, "t_fwd_kernel": t_fwd_kernel, "t_adj_kernel": t_adj_kernel,
+              "t_ode": t_ode, "hetero": W["hetero"],
+              # heterogeneous: one ODE and one summation call per trajectory chunk, each a prep + main kernel
+              "extra_launches": 3 * sum(1 for nm, *_ in spans if "traj" in nm or "ode" in nm),
               "fwd_evals": fwd_evals, "adj_evals": adj_evals, "dense_step": dense_step, "clocks": clocks,
               "e2e_t": e2e_t, "h2d": p0.nbytes + nt * ns * 4, "d2h": nt * ns * 4 + p0.nbytes,
               "levels": wpt.dyadic_decomp.num_levels, "workload": W["name"]}
@@ -308,11 +368,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cutoff", type=float, default=16.0)
-    ap.add_argument("--thr", type=int, default=65536, help="top_n (65536 = config 2; smaller for profiling)")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2",
+                    help="c2: config 2 (the headline); het512 / c3: heterogeneous media")
+    ap.add_argument("--thr", type=int, default=None, help="top_n (default: the workload's; smaller for profiling)")
     ap.add_argument("--cpu-sample", type=int, default=96)
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    if args.thr is None:
+        args.thr = DEFAULT_THR[args.workload]
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -320,6 +384,10 @@ def main():
 
     if args.impl == "reference":
         if rank != 0:
+            return 0
+        if args.workload != "c2":
+            print(json.dumps({"impl": "reference", "unavailable": "the CPU restatement of the summation covers "
+                              "homogeneous media (config 2); heterogeneous workloads have no CPU arm"}), flush=True)
             return 0
         r = cpu_reference(args)
         line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus,
@@ -344,7 +412,7 @@ def main():
     if rank != 0:
         return 0
     cpu = None
-    if not args.no_cpu_baseline and world == 1:
+    if not args.no_cpu_baseline and world == 1 and not r["hetero"]:
         try:
             cpu = cpu_reference(args)
             cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
@@ -361,7 +429,7 @@ def main():
     peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
     traffic = None
     prof = os.path.join(ROOT, "profiles", "fwd32_traffic_config2.json")
-    if os.path.exists(prof) and args.thr == 65536:
+    if os.path.exists(prof) and args.thr == 65536 and args.workload == "c2":
         with open(prof) as f:
             traffic = json.load(f).get("dram_bytes_per_launch")
     achieved = r["fwd_evals"] * flops_per_eval / r["t_fwd_kernel"] / 1e12
@@ -373,16 +441,19 @@ def main():
                    "l2": "flushed (256 MiB write) between timed steps", "cutoff_efolds": args.cutoff},
         "e2e": {"value": world * r["dense_step"] / r["e2e_t"], "unit": UNIT, "h2d_bytes_per_step": r["h2d"],
                 "d2h_bytes_per_step": r["d2h"], "ms_per_step": r["e2e_t"] * 1e3},
-        "gpu_launches": args.steps * launches_per_step(r["levels"]),
+        "gpu_launches": args.steps * launches_per_step(r["levels"]) + r["extra_launches"],
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "kernel": "fwd32_kernel", "flops_per_eval": flops_per_eval,
+                     "kernel": "fwd32_kernel<TRAJ>" if r["hetero"] else "fwd32_kernel",
+                     "flops_per_eval": flops_per_eval,
                      "peak_basis": f"148 SM x 128 FP32 lanes x 2 x {sm_mhz:.0f} MHz (median sampled SM clock)",
-                     "timing": "CUDA events around msgb_sum_fwd_f32 inside the timed steps (mean per launch)"},
+                     "timing": "CUDA events around the forward summation entry point inside the timed steps "
+                               "(device time per step, all chunks)"},
         "kernels": {"fwd32_s": r["t_fwd_kernel"], "adj32_s": r["t_adj_kernel"], "fwd_evals": r["fwd_evals"],
                     "adj_evals": r["adj_evals"], "dense_evals_per_step": r["dense_step"],
                     "fwd_evals_per_s": r["fwd_evals"] / r["t_fwd_kernel"],
-                    "adj_evals_per_s": r["adj_evals"] / r["t_adj_kernel"]},
+                    "adj_evals_per_s": r["adj_evals"] / r["t_adj_kernel"],
+                    "ode_s_per_step": r["t_ode"]},
         "clocks": clk,
         "cpu_baseline": cpu,
     }

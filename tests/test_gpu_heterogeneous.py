@@ -335,3 +335,26 @@ def test_heterogeneous_fp32_and_adjoint_dot_test():
     Aq = s64.sum_forward(s64.beams(selq, dom, wpt), dom, sens, ts).cpu().numpy()
     lhs, rhs = float(np.sum(Aq * data)), float(np.sum(q * a64))
     assert abs(lhs - rhs) <= 1e-10 * abs(lhs)
+
+
+def test_adjoint_reuses_forward_trajectories():
+    """An adjoint right after the forward (same selection, domain and time
+    grid) reads the kept trajectory records instead of integrating again; the
+    result equals the re-integrating adjoint's."""
+    import beamax_b200 as bb
+
+    _dev()
+    dom, wpt, p0, sens, ts, c, interp, thr = _het_case(seed=2, N=(64, 64), thr=60)
+    ode = bb.gb.gb_solvers.solve_ODE_base
+    for precision in ("fp64", "fp32"):
+        keep = bb.MSGBSolver(thr, "top_n", 64, "spatial", ode, "scan_real", precision=precision)
+        fresh = bb.MSGBSolver(thr, "top_n", 64, "spatial", ode, "scan_real", precision=precision,
+                              keep_trajectories=False)
+        y = keep.forward(p0, dom, sens, ts, wpt)
+        fresh.forward(p0, dom, sens, ts, wpt)
+        assert keep._cached_trajectories(keep.last_selection, dom, ts) is not None
+        assert fresh._cached_trajectories(fresh.last_selection, dom, ts) is None
+        data = np.random.default_rng(9).standard_normal(y.shape)
+        a_keep = keep.adjoint(data, dom, sens, ts, wpt)
+        a_fresh = fresh.adjoint(data, dom, sens, ts, wpt)
+        assert om.rel_l2(a_fresh, a_keep) < (1e-12 if precision == "fp64" else 1e-6)
