@@ -224,7 +224,7 @@ struct DopriBeam {
         kk[0] = f0;
         State<D> yt;
         const double *yv = vals(y);
-#pragma unroll 1
+#pragma unroll
         for (int s = 1; s < 7; ++s) {
             double *tv = vals(yt);
 #pragma unroll

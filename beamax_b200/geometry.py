@@ -154,7 +154,15 @@ class Domain:
                                   "use utils.interp.make_c_function_from_grid")
 
     def constant_speed(self) -> Optional[float]:
-        """The sound speed when the medium is homogeneous, else ``None``."""
+        """The sound speed when the medium is homogeneous, else ``None``.
+        A grid interpolant is constant exactly when its grid values are (both
+        n-linear and B-spline interpolation reproduce constants), which is
+        checked on the values without evaluating the interpolant."""
+        from .utils.interp import GridInterpolant
+
+        if isinstance(self.c, GridInterpolant):
+            v = float(self.c.values.flat[0])
+            return v if np.all(self.c.values == v) else None
         if callable(self.c):
             arr = self.sound_speed_array
             v = float(arr.flat[0])

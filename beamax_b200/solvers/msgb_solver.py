@@ -205,10 +205,9 @@ class MSGBSolver:
     def _problem(self, domain: Domain, sensors, ts, device):
         import torch
 
-        c = domain.constant_speed()
-        if c is None:
-            c = domain.compute_max_speed()  # unused by the trajectory kernels
-        elif domain.lam != 0.0:
+        kind, m = domain.medium()
+        c = float(m) if kind == "constant" else float(np.max(m.values))  # unused by the trajectory kernels
+        if kind == "constant" and domain.lam != 0.0:
             raise NotImplementedError("absorption (lam != 0) needs the ODE path (heterogeneous media)")
         pos = np.ascontiguousarray(self._sensor_positions(sensors), np.float64)
         if pos.ndim != 2 or pos.shape[1] != domain.ndim:
