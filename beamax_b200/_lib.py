@@ -31,7 +31,7 @@ class Problem(ctypes.Structure):
 
 class BeamSet(ctypes.Structure):
     _fields_ = [("n", c_i64), ("x0", c_vp), ("p0", c_vp), ("alpha", c_vp), ("a0", c_vp),
-                ("omega", c_vp)]
+                ("omega", c_vp), ("modes", c_i32)]
 
 
 class SensorTiling(ctypes.Structure):
@@ -99,6 +99,8 @@ SIGNATURES = {
     "msgb_rk4_trajectories": (ctypes.c_int, [c_vp, c_vp, c_vp, ctypes.c_int, c_vp, c_vp]),
     "msgb_ode_trajectories": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "msgb_threshold_workspace_size": (c_sz, [c_i64]),
+    "msgb_coefficients_dpdt": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_int, ctypes.c_int, c_vp, c_vp,
+                                              c_vp]),
     "msgb_threshold": (ctypes.c_int, [ctypes.c_int, c_dbl, c_vp, c_vp, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_sz,
                                       c_vp]),
     "msgb_surrogate_features": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),

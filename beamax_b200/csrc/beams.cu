@@ -12,7 +12,7 @@
 // _coefficient_positions (forward_solver_utils.py:233-252).
 #include <cub/cub.cuh>
 
-#include "common.cuh"
+#include "traj.cuh"
 
 // Layout shared with mswpt.cu (only the fields read here).
 struct msgb_mswpt;
@@ -134,6 +134,64 @@ __global__ void beam_init_kernel(InitArgs A) {
     A.out.omega[i] = norm;
 }
 
+// compute_coefficients with an initial time derivative
+// (forward_solver_utils.py:716-786): c = 0.5 (a + branch i b / vg) with
+// vg = G(x_b, p_b, +1) = c(x_b) |p_b| (gb_utils.py:11-44), x_b the
+// coefficient's position (_coefficient_positions) and p_b = 2 pi centre / L
+// its box's centre frequency.
+struct DpdtArgs {
+    PlanView v;
+    double L[3];
+    MediumArgs med;
+    const double2 *a, *b;
+    int64_t total;
+    double branch;
+    int mask;
+    double2 *out;
+    double *keys;
+};
+
+template <int D>
+__global__ void dpdt_kernel(DpdtArgs A) {
+    const int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (f >= A.total) return;
+    const PlanView &v = A.v;
+    int l = 0;
+    while (l < v.levels - 1 && f >= v.ccum[l + 1]) ++l;
+    const int64_t local = f - v.ccum[l];
+    int S[3] = {1, 1, 1};
+    int64_t P = 1;
+    for (int a = 0; a < D; ++a) {
+        S[a] = 2 * v.bshape[l][a];
+        P *= S[a];
+    }
+    const int64_t box_local = local / P;
+    int64_t rem = local - box_local * P;
+    int k[3] = {0, 0, 0};
+    for (int a = D - 1; a >= 0; --a) {
+        k[a] = (int)(rem % S[a]);
+        rem /= S[a];
+    }
+    const int64_t box = v.bcum[l] + box_local;
+    double x[D], p2 = 0.0;
+    for (int a = 0; a < D; ++a) {
+        const int support = v.bl[l] * v.red * v.aspect[a];
+        x[a] = (double)k[a] * A.L[a] / (double)support;
+        const double pb = 2.0 * 3.141592653589793 * (double)v.centres[box * D + a] / A.L[a];
+        p2 += pb * pb;
+    }
+    double c, g[D], H[D * D];
+    speed_eval<D>(A.med, x, c, g, H);
+    const double vg = c * sqrt(p2);
+    const double2 ca = A.a[f], cb = A.b[f];
+    // i b / vg = (-b.im, b.re) / vg
+    double re = 0.5 * (ca.x - A.branch * cb.y / vg);
+    double im = 0.5 * (ca.y + A.branch * cb.x / vg);
+    if (A.mask && local >= (v.ccum[l + 1] - v.ccum[l]) / 2) re = im = 0.0;
+    A.out[f] = make_double2(re, im);
+    if (A.keys) A.keys[f] = sqrt(__dadd_rn(__dmul_rn(re, re), __dmul_rn(im, im)));
+}
+
 struct ScatterArgs {
     const int64_t *idx;
     const double2 *g;
@@ -232,6 +290,36 @@ extern "C" int msgb_beam_init(const msgb_mswpt *plan, const double *L, const int
     A.out = *out;
     beam_init_kernel<<<(unsigned)((n + 255) / 256), 256, 0, as_stream(stream)>>>(A);
     return check_launch("msgb_beam_init");
+}
+
+extern "C" int msgb_coefficients_dpdt(const msgb_mswpt *plan, const double *L, const msgb_medium *med,
+                                      const double *a, const double *b, int branch, int apply_half_mask,
+                                      double *out, double *keys, msgb_stream_t stream) {
+    if (!plan || !L || !med || !a || !b || !out) return fail(MSGB_ERR_ARG, "msgb_coefficients_dpdt: NULL argument");
+    if (branch != 1 && branch != -1) return fail(MSGB_ERR_ARG, "branch must be +1 or -1");
+    DpdtArgs A{};
+    if (int e = plan_view(plan, A.v)) return e;
+    for (int i = 0; i < 3; ++i) A.L[i] = i < A.v.nd ? L[i] : 1.0;
+    msgb_problem pr{};
+    pr.ndim = A.v.nd;
+    if (int e = medium_args(&pr, med, A.med)) return e;
+    A.a = (const double2 *)a;
+    A.b = (const double2 *)b;
+    A.total = A.v.ccum[A.v.levels];
+    A.branch = (double)branch;
+    A.mask = apply_half_mask;
+    A.out = (double2 *)out;
+    A.keys = keys;
+    if (A.total == 0) return MSGB_OK;
+    const int blk = 256;
+    const unsigned grid = (unsigned)((A.total + blk - 1) / blk);
+    cudaStream_t st = as_stream(stream);
+    switch (A.v.nd) {
+        case 1: dpdt_kernel<1><<<grid, blk, 0, st>>>(A); break;
+        case 2: dpdt_kernel<2><<<grid, blk, 0, st>>>(A); break;
+        default: dpdt_kernel<3><<<grid, blk, 0, st>>>(A); break;
+    }
+    return check_launch("msgb_coefficients_dpdt");
 }
 
 extern "C" int msgb_scatter_coeff_grad(const int64_t *idx, const double *g, int64_t n, double scale,

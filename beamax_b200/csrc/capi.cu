@@ -48,6 +48,7 @@ int validate_beams(const msgb_problem *p, const msgb_beam_set *b) {
     if (b->n < 0) return fail(MSGB_ERR_ARG, "negative beam count");
     if (b->n > 0 && (!b->x0 || !b->p0 || !b->alpha || !b->a0 || !b->omega))
         return fail(MSGB_ERR_ARG, "beam arrays must not be NULL");
+    if (b->modes < 0 || b->modes > 2) return fail(MSGB_ERR_ARG, "beam modes must be 0, 1 or 2");
     return MSGB_OK;
 }
 
@@ -74,6 +75,7 @@ BeamArgs to_args(const msgb_beam_set *b) {
     a.alpha = b->alpha;
     a.a0 = b->a0;
     a.omega = b->omega;
+    a.modes = b->modes;
     return a;
 }
 

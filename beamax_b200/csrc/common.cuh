@@ -155,7 +155,10 @@ struct ProbArgs {
 struct BeamArgs {
     int64_t n;
     const double *x0, *p0, *alpha, *a0, *omega;
+    int modes;  // 0 both branches, 1 only mode +1, 2 only mode -1
 };
+
+__host__ __device__ __forceinline__ bool mode_on(int modes, int m) { return modes == 0 || modes == m + 1; }
 
 int validate_problem(const msgb_problem *p);
 int validate_beams(const msgb_problem *p, const msgb_beam_set *b);

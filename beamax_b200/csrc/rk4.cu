@@ -208,7 +208,10 @@ struct DopriBeam {
         constexpr int NE = 2 * D + D * D + 1;
         static_assert(sizeof(State<D>) == N * sizeof(double), "State<D> must be a plain array of doubles");
         if (k >= P.nt) return true;
-        if (steps >= o.max_steps) {
+        // Ending steps on the save times adds up to nt - 1 steps that an
+        // integrator reading an interpolant would not take; they do not count
+        // against the budget.
+        if (steps >= o.max_steps + (o.dense_output ? 0 : P.nt - 1)) {
             code = 2;
             return true;
         }

@@ -604,8 +604,8 @@ fwd32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
                     keep_p = traj_survives<D>(T, j, tt, ti, cutoff);
                 } else {
                     const Cull<D> cb = cull[j];
-                    keep_p = survives<D>(cb, (float)P.c, ta, tb, ti, P, cutoff);
-                    keep_m = survives<D>(cb, -(float)P.c, ta, tb, ti, P, cutoff);
+                    keep_p = mode_on(B.modes, 0) && survives<D>(cb, (float)P.c, ta, tb, ti, P, cutoff);
+                    keep_m = mode_on(B.modes, 1) && survives<D>(cb, -(float)P.c, ta, tb, ti, P, cutoff);
                 }
             }
             const unsigned bp = __ballot_sync(0xffffffffu, keep_p);
@@ -738,6 +738,7 @@ adj32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
     const int64_t n_tt = (P.nt + TT - 1) / TT;
     double gre = 0.0, gim = 0.0;
     for (int m = 0; m < (TRAJ ? 1 : 2); ++m) {
+        if (!TRAJ && !mode_on(B.modes, m)) continue;
         const float c0 = m == 0 ? (float)P.c : -(float)P.c;
         const int64_t b = m == 0 ? j : j + B.n;
         for (int64_t tt = 0; tt < n_tt; ++tt) {

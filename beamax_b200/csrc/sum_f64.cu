@@ -117,8 +117,9 @@ __global__ void __launch_bounds__(THREADS) fwd64_kernel(ProbArgs P, BeamArgs B, 
 #pragma unroll
     for (int k = 0; k < TPT; ++k) acc[k] = 0.0;
 
-    const int64_t nb = 2 * B.n;
-    for (int64_t b0 = 0; b0 < nb; b0 += BC) {
+    const int64_t nb = B.modes == 1 ? B.n : 2 * B.n;        // end of the summed beams
+    const int64_t b_lo = B.modes == 2 ? B.n : 0;             // start
+    for (int64_t b0 = b_lo; b0 < nb; b0 += BC) {
         {
             const int bl = tid / TT, tl = tid % TT;
             const int64_t b = b0 + bl;
@@ -170,6 +171,7 @@ __global__ void __launch_bounds__(THREADS) adj64_kernel(ProbArgs P, BeamArgs B, 
     load_beam<D>(B, j, x0, p0, al, a0, w);
     double acc_re = 0.0, acc_im = 0.0;
     for (int m = 0; m < 2; ++m) {
+        if (!mode_on(B.modes, m)) continue;
         const double c0 = m == 0 ? P.c : -P.c;
         for (int64_t t = warp; t < P.nt; t += THREADS / 32) {
             HomState<D> st;

@@ -26,7 +26,7 @@ from __future__ import annotations
 import contextlib
 import ctypes
 import math
-from dataclasses import dataclass
+from dataclasses import dataclass, replace
 from numbers import Integral, Real
 from typing import Optional, Tuple
 
@@ -68,6 +68,19 @@ class Selection:
 
 
 @dataclass
+class BranchSelection:
+    """The complex-input path's two selections (msgb_solver.py:635-689): c_pos
+    coefficients drive mode +1 beams, c_neg coefficients mode -1 beams."""
+
+    pos: Selection
+    neg: Selection
+
+    @property
+    def total_coeffs(self) -> int:
+        return self.pos.total_coeffs
+
+
+@dataclass
 class BeamTensors:
     x0: "object"
     p0: "object"
@@ -75,6 +88,7 @@ class BeamTensors:
     a0: "object"       # complex128 (n,)
     a0_unit: "object"  # complex128 (n,)
     omega: "object"
+    modes: int = 0     # 0 both branches (mirrored), 1 only mode +1, 2 only mode -1
 
     @property
     def n(self) -> int:
@@ -86,7 +100,12 @@ class BeamTensors:
         a0 = self.a0_unit if unit else self.a0
         return _lib.BeamSet(n=self.n, x0=self.x0.data_ptr(), p0=self.p0.data_ptr(),
                             alpha=torch.view_as_real(self.alpha).data_ptr(),
-                            a0=torch.view_as_real(a0).data_ptr(), omega=self.omega.data_ptr())
+                            a0=torch.view_as_real(a0).data_ptr(), omega=self.omega.data_ptr(), modes=self.modes)
+
+    def with_amplitude(self, factor, modes=None):
+        """The same beams with a0 and a0_unit multiplied by ``factor``."""
+        return BeamTensors(self.x0, self.p0, self.alpha, self.a0 * factor, self.a0_unit * factor, self.omega,
+                           self.modes if modes is None else modes)
 
 
 class MSGBSolver:
@@ -259,18 +278,37 @@ class MSGBSolver:
         import torch
 
         x = as_device_f64(p0)
-        if x.is_complex():
-            raise NotImplementedError("complex p0 (the *_complex parameter path) is not implemented")
+        dz = None
         if dpdt is not None:
-            dz = dpdt.detach() if hasattr(dpdt, "detach") else np.asarray(dpdt)
-            nonzero = bool((dz != 0).any()) if hasattr(dz, "any") else bool(np.any(dz))
-            if nonzero:
-                raise NotImplementedError("non-zero dpdt is not implemented on the GPU path")
-        coeffs, keys = wpt.forward_device(x, self.input_type, scale=0.5, half_mask=True, keys=True)
+            dz = as_device_f64(dpdt, x.device)
+            if not bool((dz != 0).any()):
+                dz = None
+        if x.is_complex() or (dz is not None and dz.is_complex()):
+            return self._select_branches(x, dz, domain, wpt)
+        if dz is None:
+            coeffs, keys = wpt.forward_device(x, self.input_type, scale=0.5, half_mask=True, keys=True)
+        else:
+            coeffs, keys = self._coefficients_dpdt(x, dz, domain, wpt, branch=1, half_mask=True)
+        return self._select_from(coeffs, keys, wpt, x.device, self._effective_top_n(wpt, half_frame=True))
+
+    def _select_branches(self, x, dz, domain: Domain, wpt: MSWPT) -> BranchSelection:
+        """Complex input (msgb_solver.py:635-689): c_pos and c_neg of
+        compute_coefficients(mode="both") thresholded separately with the
+        uncapped top_n (no half-frame mask)."""
+        if dz is None:
+            c, k = wpt.forward_device(x, self.input_type, scale=0.5, keys=True)
+            cp, kp, cn, kn = c, k, c, k
+        else:
+            cp, kp = self._coefficients_dpdt(x, dz, domain, wpt, branch=1, half_mask=False)
+            cn, kn = self._coefficients_dpdt(x, dz, domain, wpt, branch=-1, half_mask=False)
+        n = self._effective_top_n(wpt)
+        return BranchSelection(self._select_from(cp, kp, wpt, x.device, n), self._select_from(cn, kn, wpt, x.device, n))
+
+    def _select_from(self, coeffs, keys, wpt: MSWPT, dev, n) -> Selection:
+        import torch
+
         if self.thr_strat != "top_n":
-            return self._select_masked(coeffs, keys, wpt, x.device)
-        n = self._effective_top_n(wpt, half_frame=True)
-        dev = x.device
+            return self._select_masked(coeffs, keys, wpt, dev)
         idx = torch.empty(n, dtype=torch.int64, device=dev)
         vals = torch.empty(n, dtype=torch.complex128, device=dev)
         nbytes = _lib.lib().msgb_topn_workspace_size(wpt.total_coeffs, n)
@@ -280,6 +318,26 @@ class MSGBSolver:
                                         n, idx.data_ptr(), torch.view_as_real(vals).data_ptr(), ws.data_ptr(),
                                         nbytes, st), "msgb_topn")
         return Selection(idx, vals, wpt.total_coeffs)
+
+    def _coefficients_dpdt(self, x, dz, domain: Domain, wpt: MSWPT, branch: int, half_mask: bool):
+        """c = 0.5 (MSWPT(p0) + branch i MSWPT(dpdt) / vg) and its keys
+        (forward_solver_utils.py:716-786) via msgb_coefficients_dpdt."""
+        import torch
+
+        dev = x.device
+        a = wpt.forward_device(x, self.input_type, scale=1.0)
+        b = wpt.forward_device(dz, self.input_type, scale=1.0)
+        med, keep_m = self._medium(domain, dev)
+        d = domain.ndim
+        L = (ctypes.c_double * 3)(*[float(v) for v in domain.grid_size], *([1.0] * (3 - d)))
+        out = torch.empty_like(a)
+        keys = torch.empty(a.shape[0], dtype=torch.float64, device=dev)
+        st = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(_lib.lib().msgb_coefficients_dpdt(wpt.plan(dev), L, _lib.ref(med), torch.view_as_real(a).data_ptr(),
+                                                     torch.view_as_real(b).data_ptr(), int(branch), int(half_mask),
+                                                     torch.view_as_real(out).data_ptr(), keys.data_ptr(), st),
+                   "msgb_coefficients_dpdt")
+        return out, keys
 
     _THR_CODE = {"hard": 0, "percentile": 1, "hard_reassign": 2, "bao_energy": 3, "perc_max_abs": 4}
 
@@ -370,6 +428,14 @@ class MSGBSolver:
                             dt0=float(cfg.dt0) if cfg.dt0 is not None else 0.0, max_steps=int(cfg.max_steps),
                             dense_output=int(bool(cfg.dense_output)))
 
+    def _mode_chunks(self, domain: Domain, nt: int, bt: BeamTensors, fp64: bool):
+        """Chunks over the beams of the summed branches: [0, 2n), [0, n) (mode
+        +1 only) or [n, 2n) (mode -1 only)."""
+        n = bt.n
+        lo, hi = {0: (0, 2 * n), 1: (0, n), 2: (n, 2 * n)}[bt.modes]
+        chunks, per, n_tt = self._chunks(domain, nt, hi - lo, fp64)
+        return [(lo + b, nb) for b, nb in chunks], per, n_tt
+
     def _trajectories(self, pr, med, bs, b_first, nb, fp64, per, n_tt, dev, st, status, buf=None):
         if buf is None:
             buf = workspace(dev, "traj", per * nb + 4096)
@@ -434,7 +500,7 @@ class MSGBSolver:
         bs = bt.beam_set(unit=False)
         st = torch.cuda.current_stream(dev).cuda_stream
         fp64 = self.precision == "fp64"
-        chunks, per, n_tt = self._chunks(domain, pr.nt, 2 * bt.n, fp64)
+        chunks, per, n_tt = self._mode_chunks(domain, pr.nt, bt, fp64)
         status = torch.zeros(2 * bt.n, dtype=torch.int32, device=dev)
         self._begin_trajectories(domain, ts)
         self._traj_cache = None
@@ -492,8 +558,8 @@ class MSGBSolver:
         st = torch.cuda.current_stream(dev).cuda_stream
         fp64 = self.precision == "fp64"
         n = bt.n
-        chunks, per, n_tt = self._chunks(domain, pr.nt, 2 * n, fp64)
-        g_all = torch.empty(2 * n, dtype=torch.complex128, device=dev)
+        chunks, per, n_tt = self._mode_chunks(domain, pr.nt, bt, fp64)
+        g_all = torch.zeros(2 * n, dtype=torch.complex128, device=dev)
         if fp64:
             d = as_device_f64(data, dev).reshape(pr.nt, pr.ns).contiguous()
         elif isinstance(data, torch.Tensor) and data.is_cuda and data.dtype == torch.float32:
@@ -613,8 +679,6 @@ class MSGBSolver:
         if wpt.dyadic_decomp.N != domain.N:
             raise ValueError("wpt grid shape must match domain.N.")
         _validate_time_grid(ts, allow_singleton=True)
-        if not self.use_real:
-            raise NotImplementedError(f"sum_method={self.sum_method!r}: complex summation is not implemented")
 
     def forward(self, p0, domain: Domain, sensors, ts, wpt: MSWPT, *, dpdt=None):
         """Pressure at the sensors, shape (Nt, Ns) (msgb_solver.py:858-899)."""
@@ -627,9 +691,16 @@ class MSGBSolver:
         The coefficients of p0 at S's indices drive S's beams."""
         self._check_forward_args(p0, domain, ts, wpt, None)
         x = as_device_f64(p0)
-        c = wpt.forward_device(x, self.input_type, scale=0.5, half_mask=True)
-        sel = Selection(selection.idx, c[selection.idx], selection.total_coeffs)
-        out = self.sum_forward(self.beams(sel, domain, wpt), domain, sensors, ts)
+        if isinstance(selection, BranchSelection):
+            c = wpt.forward_device(x, self.input_type, scale=0.5)
+            take = lambda s: Selection(s.idx, c[s.idx], s.total_coeffs)
+            bts = [replace(self.beams(take(selection.pos), domain, wpt), modes=1),
+                   replace(self.beams(take(selection.neg), domain, wpt), modes=2)]
+        else:
+            c = wpt.forward_device(x, self.input_type, scale=0.5, half_mask=True)
+            sel = Selection(selection.idx, c[selection.idx], selection.total_coeffs)
+            bts = [self.beams(sel, domain, wpt)]
+        out = self._sum_beam_sets(bts, domain, sensors, ts)
         return out if _is_torch(p0) else out.cpu().numpy()
 
     def forward_with_params(self, p0, domain: Domain, sensors, ts, wpt: MSWPT, *, dpdt=None):
@@ -642,29 +713,50 @@ class MSGBSolver:
         self._check_forward_args(p0, domain, ts, wpt, dpdt)
         self._sensor_positions(sensors)
         sel = self.select(p0, domain, wpt, dpdt)
-        bt = self.beams(sel, domain, wpt)
-        self._traj_owner = sel
+        if isinstance(sel, BranchSelection):
+            bts = [replace(self.beams(sel.pos, domain, wpt), modes=1), replace(self.beams(sel.neg, domain, wpt), modes=2)]
+        else:
+            bts = [self.beams(sel, domain, wpt)]
+        self._traj_owner = sel if (len(bts) == 1 and self.use_real) else None
         try:
-            out = self.sum_forward(bt, domain, sensors, ts)
+            out = self._sum_beam_sets(bts, domain, sensors, ts)
         finally:
             self._traj_owner = None
         self.last_selection = sel
         result = out if _is_torch(p0) else out.cpu().numpy()
         if not want_params:
             return result, None
-        return result, self._params_like_reference(bt, domain, as_numpy=not _is_torch(p0))
+        return result, self._params_like_reference(bts, domain, as_numpy=not _is_torch(p0))
 
-    def _params_like_reference(self, bt: BeamTensors, domain: Domain, as_numpy: bool):
+    def _sum_beam_sets(self, bts, domain: Domain, sensors, ts):
+        """Sum over beam sets: the real field sum_b 2 Re(a0 K_b) (scan_real,
+        gb/core.py:194-329) or, for the *_complex sum methods, the complex
+        field sum_b a0 K_b (gb/core.py:105-168), which is
+        0.5 (S(a0) + i S(-i a0)) with S the real summation."""
+        total = None
+        for bt in bts:
+            part = self.sum_forward(bt, domain, sensors, ts)
+            if not self.use_real:
+                im = self.sum_forward(bt.with_amplitude(-1j), domain, sensors, ts)
+                part = 0.5 * (part + 1j * im)
+            total = part if total is None else total + part
+        return total
+
+    def _params_like_reference(self, bts, domain: Domain, as_numpy: bool):
         import torch
 
         d = domain.ndim
-        eye = torch.eye(d, dtype=torch.complex128, device=bt.alpha.device)
-        M0 = bt.alpha[:, :, None] * eye
-        cat = lambda t: torch.cat([t, t], 0)
-        n = bt.n
-        modes = torch.cat([torch.ones(n, dtype=torch.float64, device=bt.omega.device),
-                           -torch.ones(n, dtype=torch.float64, device=bt.omega.device)])
-        params = [cat(bt.p0), cat(M0), cat(bt.x0), cat(bt.omega), cat(bt.a0), modes]
+        if len(bts) == 1:  # real input: the selection mirrored over both modes
+            bt = bts[0]
+            parts = [(bt, 1.0), (bt, -1.0)]
+        else:              # complex input: c_pos beams (+1), then c_neg beams (-1)
+            parts = [(bts[0], 1.0), (bts[1], -1.0)]
+        dev = bts[0].omega.device
+        eye = torch.eye(d, dtype=torch.complex128, device=dev)
+        cat = lambda f: torch.cat([f(bt) for bt, _ in parts], 0)
+        modes = torch.cat([torch.full((bt.n,), m, dtype=torch.float64, device=dev) for bt, m in parts])
+        params = [cat(lambda b: b.p0), cat(lambda b: b.alpha[:, :, None] * eye), cat(lambda b: b.x0),
+                  cat(lambda b: b.omega), cat(lambda b: b.a0), modes]
         if self.aggregate_method in ("scan", "vmap"):
             b = params[0].shape[0]
             nb = (b + self.batch_size - 1) // self.batch_size
@@ -707,6 +799,15 @@ class MSGBSolver:
                 selection = self.last_selection
             else:
                 raise ValueError("adjoint needs a beam selection: call forward first or pass p0= or selection=")
+        complex_data = _is_complex(data)
+        if complex_data and self.use_real:
+            raise ValueError("complex data needs a *_complex sum_method (the real path's output is real)")
+        if isinstance(selection, BranchSelection):
+            if self.use_real:
+                raise NotImplementedError("the adjoint of the complex-input path with a real sum_method "
+                                          "(a map from complex images to real data) is not implemented")
+            img = self._adjoint_branches(data, domain, sensors, ts, wpt, selection)
+            return img if _is_torch(data) else img.cpu().numpy()
         # Gather in flat-index order: neighbouring coefficients (same box,
         # adjacent packet positions) have overlapping footprints, so the
         # per-beam warps of a CTA reuse the same data tiles from L1.
@@ -717,9 +818,41 @@ class MSGBSolver:
             order = torch_argsort(selection.idx)
             sel_sorted = Selection(selection.idx[order], selection.values[order], selection.total_coeffs)
         bt = self.beams(sel_sorted, domain, wpt)
-        g = self.gather_adjoint(bt, domain, sensors, ts, data, cached)
+        if complex_data:
+            g = self._gather_complex(bt, domain, sensors, ts, data)
+        else:
+            g = self.gather_adjoint(bt, domain, sensors, ts, data, cached)
         img = self.coefficient_adjoint(sel_sorted, g, wpt)
         return img if _is_torch(data) else img.cpu().numpy()
+
+    def _gather_complex(self, bt: BeamTensors, domain: Domain, sensors, ts, data):
+        """Hermitian gather for complex data: g_j = sum conj(a0u_j K_j) d
+        = 0.5 (G(Re d) + i G(Im d)), G the real gather (sum 2 d conj(a0u K))."""
+        d = as_device_f64(data, bt.x0.device)
+        gr = self.gather_adjoint(bt, domain, sensors, ts, d.real.contiguous())
+        gi = self.gather_adjoint(bt, domain, sensors, ts, d.imag.contiguous())
+        return 0.5 * (gr + 1j * gi)
+
+    def _adjoint_branches(self, data, domain: Domain, sensors, ts, wpt: MSWPT, selection: BranchSelection):
+        """Hermitian adjoint of the complex-input forward (c_pos beams mode +1,
+        c_neg beams mode -1, complex sum): both branches' coefficients are
+        0.5 MSWPT(p0) (the dpdt term does not depend on p0), so the image is
+        MSWPT^H(0.5 (scatter g_pos + scatter g_neg)), complex."""
+        import torch
+
+        dev = selection.pos.idx.device
+        G = torch.zeros(wpt.total_coeffs, dtype=torch.complex128, device=dev)
+        st = torch.cuda.current_stream(dev).cuda_stream
+        for sel, modes in ((selection.pos, 1), (selection.neg, 2)):
+            order = torch_argsort(sel.idx)
+            s_sorted = Selection(sel.idx[order], sel.values[order], sel.total_coeffs)
+            bt = replace(self.beams(s_sorted, domain, wpt), modes=modes)
+            g = self._gather_complex(bt, domain, sensors, ts, data)
+            _lib.check(_lib.lib().msgb_scatter_coeff_grad(s_sorted.idx.data_ptr(), torch.view_as_real(g).data_ptr(),
+                                                          int(s_sorted.idx.shape[0]), 0.5, wpt.plan(dev), 0,
+                                                          torch.view_as_real(G).data_ptr(), st),
+                       "msgb_scatter_coeff_grad")
+        return wpt.adjoint(G, "spatial", real_output=False)
 
     def eval_count(self) -> Optional[int]:
         """Evaluated (beam, time, sensor) triples of the last FP32 call."""
@@ -735,3 +868,7 @@ def torch_argsort(x):
 
 def _is_torch(x) -> bool:
     return hasattr(x, "detach") and hasattr(x, "device")
+
+
+def _is_complex(x) -> bool:
+    return x.is_complex() if _is_torch(x) else np.iscomplexobj(x)

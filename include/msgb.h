@@ -67,6 +67,10 @@ typedef struct msgb_beam_set {
     const double *a0;        /* (n) complex: amplitude; includes the coefficient for
                                 the forward, the unit amplitude for the adjoint */
     const double *omega;     /* (n) frequency |xi| */
+    int32_t modes;           /* which of the two branches are summed: 0 both (beam b < n
+                                mode +1, b >= n mode -1, the real path's mirrored set),
+                                1 only mode +1, 2 only mode -1 (the complex path's two
+                                selections); homogeneous summations only */
 } msgb_beam_set;
 
 /* Optional sensor order for the FP32 summation (device pointers).  Tile i
@@ -204,7 +208,8 @@ typedef struct msgb_ode_opts {
     int32_t substeps;        /* RK4 */
     double rtol, atol;       /* DOPRI5: error norm RMS |e| / (atol + rtol max(|y0|, |y1|)) */
     double dt0;              /* DOPRI5 first step; <= 0 selects ts[1] - ts[0] */
-    int64_t max_steps;       /* DOPRI5: accepted + rejected steps per beam */
+    int64_t max_steps;       /* DOPRI5: accepted + rejected steps per beam (plus nt - 1
+                                when steps end on the save times) */
     int32_t only_flagged;    /* nonzero: integrate only beams whose out->status entry is
                                 nonzero (e.g. rejected surrogate predictions); the
                                 records of the others are left as they are */
@@ -423,6 +428,17 @@ typedef struct msgb_beam_out {
 int msgb_beam_init(const msgb_mswpt *plan, const double *L, const int64_t *idx,
                    const double *values, int64_t n, const msgb_beam_out *out,
                    msgb_stream_t stream);
+
+/* compute_coefficients with a non-zero initial time derivative
+ * (forward_solver_utils.py:716-786): from a = MSWPT(p0) and b = MSWPT(dpdt)
+ * (complex, unscaled), out = 0.5 (a + branch i b / vg) with
+ * vg = c(x_b) |2 pi centre / L| per coefficient (gb_utils.py:11-44; x_b the
+ * coefficient's position, c from the medium), branch +1 (c_pos) or -1
+ * (c_neg); with apply_half_mask the second half of every level is zeroed.
+ * keys (optional): |out| for the selection.  L: host array of ndim lengths. */
+int msgb_coefficients_dpdt(const msgb_mswpt *plan, const double *L, const msgb_medium *med,
+                           const double *a, const double *b, int branch, int apply_half_mask,
+                           double *out, double *keys, msgb_stream_t stream);
 
 /* ---- adjoint scatter to coefficient space ------------------------------ */
 

@@ -272,7 +272,8 @@ def dopri5(x0, p0, M0, a0, mode, ts, speed, lam=0.0, rtol=1e-7, atol=1e-9, max_s
     and save times inside a step are read from the continuous extension
     (``dense_state``), as diffrax's SaveAt(ts) reads its solver's interpolant.
     ``max_steps`` counts accepted and rejected steps over the whole solve, as
-    diffrax does (gb/gb_solvers.py:756-783 builds that solve: Tsit5,
+    diffrax does (plus nt - 1 when steps end on the save times, the steps a
+    solver reading its interpolant would not take) (gb/gb_solvers.py:756-783 builds that solve: Tsit5,
     PIDController(rtol, atol), SaveAt(ts), dt0 = ts[1] - ts[0]).
     Returns (xt, pt, Mt, At, status, steps); status 0 ok, 1 non-finite,
     2 max_steps reached (later save times then hold the last state).
@@ -289,8 +290,9 @@ def dopri5(x0, p0, M0, a0, mode, ts, speed, lam=0.0, rtol=1e-7, atol=1e-9, max_s
     t = ts[0]
     k = 1
     rejected = False
+    budget = max_steps + (0 if dense else nt - 1)  # landings on save times do not count
     while k < nt and status == 0:
-        if steps >= max_steps:
+        if steps >= budget:
             status = 2
             break
         target = ts[-1] if dense else ts[k]

@@ -213,20 +213,21 @@ def test_dopri5_accuracy_against_dop853():
 
 
 def test_dopri5_step_budget_reports_status_and_solver_raises():
-    """max_steps counts accepted and rejected steps; running out leaves status
-    2 (the host raises, as diffeqsolve does) without touching other beams."""
+    """max_steps counts accepted and rejected steps (with the continuous
+    extension; ending steps on the save times adds nt - 1); running out leaves
+    status 2 (the host raises, as diffeqsolve does)."""
     import beamax_b200 as bb
 
     N, dx = (64, 64), (1e-4, 1e-4)
     c, interp = _random_medium(N, dx, 0.1, 6.0, 3)
     n, x0, p0, alpha = _beams3()
     ts = np.arange(0, 80) * 2e-8
-    rec, stat = _rk4_states(2, x0, p0, alpha, ts, _grid_medium(interp), (64e-4, 64e-4), ode=_dopri(max_steps=10),
-                            status=True)
+    rec, stat = _rk4_states(2, x0, p0, alpha, ts, _grid_medium(interp), (64e-4, 64e-4),
+                            ode=_dopri(max_steps=10, dense=True), status=True)
     assert (stat == 2).all()
     assert np.isfinite(rec).all()
     dom, wpt, p0g, sens, tsg, c2, interp2, thr = _het_case(thr=4)
-    cfg = bb.gb.gb_solvers.SolverConfig(max_steps=3)
+    cfg = bb.gb.gb_solvers.SolverConfig(max_steps=3, dense_output=True)
     solver = bb.MSGBSolver(thr, "top_n", 64, "spatial", bb.gb.gb_solvers.solve_ODE_base, "scan_real", ode_config=cfg)
     with pytest.raises(RuntimeError, match="max_steps"):
         solver.forward(p0g, dom, sens, tsg, wpt)

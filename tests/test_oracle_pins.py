@@ -295,5 +295,8 @@ def test_oracle_dopri5_converges_to_dop853_and_honours_max_steps():
         assert status == 0
         errs.append(np.max(np.abs(M - Mt)) / np.max(np.abs(Mt)))
     assert errs[1] < 0.1 * errs[0]
-    *_, status, steps = oo.dopri5(x0, p0, M0, 1.0, 1.0, ts, speed, max_steps=5)
+    *_, status, steps = oo.dopri5(x0, p0, M0, 1.0, 1.0, ts, speed, max_steps=5, dense=True)
     assert status == 2 and steps == 5
+    # ending steps on the save times adds nt - 1 to the budget
+    *_, status, steps = oo.dopri5(x0, p0, M0, 1.0, 1.0, ts, speed, max_steps=2)
+    assert status == 2 and steps == 2 + ts.size - 1
