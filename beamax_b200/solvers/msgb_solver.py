@@ -132,7 +132,7 @@ class MSGBSolver:
     def __init__(self, thr, thr_strat: str, batch_size: int, input_type: str, ode_solver, sum_method: str,
                  tr_ode_solver=None, sharding=None, ode_config=None, adjoint_relative_guard: float = 5e-2,
                  *, precision: str = "fp64", cutoff: float = 16.0, rk4_substeps: int = 1,
-                 trajectory_memory: int = 40 << 30, surrogate=None, keep_trajectories: bool = True):
+                 trajectory_memory: int = 48 << 30, surrogate=None, keep_trajectories: bool = True):
         valid_thresholds = {"hard", "top_n", "percentile", "hard_reassign", "bao_energy", "perc_max_abs"}
         if thr_strat not in valid_thresholds:
             raise ValueError(f"thr_strat must be one of {', '.join(sorted(valid_thresholds))}; got {thr_strat!r}.")

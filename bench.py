@@ -20,11 +20,12 @@ per second of forward + adjoint (2 * 2n * Nt * Ns per step / step time).
 (C/OpenMP FP64, dense, all host threads) on a bounded beam sample and
 reports the same metric.
 
-``--workload het512`` / ``c3`` measure the heterogeneous path instead
+``--workload het512`` / ``c3`` / ``c5`` measure the heterogeneous path instead
 (seeded random sound speed, adaptive FP64 beam ODE, trajectory summation):
 het512 is config 2's geometry in a 20-cell-correlation medium, c3 the 1024^2,
 dx 5e-5, 40-cell-correlation configuration with the valid 4-level tiling and
-thr 262,144 (its dense FP64 comparison takes minutes).
+thr 262,144, c5 the 3D 128^3 configuration (their dense FP64 comparisons take
+minutes).
 """
 
 from __future__ import annotations
@@ -54,14 +55,25 @@ def level_annuli(N, nbl, nl):
     return [nbl[l] * bls[l] / 2 for l in range(nl)]
 
 
+def _window(N, c, radius):
+    """Index ranges of the box of half-width ``radius`` around ``c``, clipped."""
+    return tuple(slice(max(0, int(np.floor(ci - radius))), min(n, int(np.ceil(ci + radius)) + 1))
+                 for ci, n in zip(c, N))
+
+
 def make_p0(N, nbl, n_packets, n_blobs, blob_sigma, seed):
+    """Seeded packets and blobs; each Gaussian is evaluated within 9 widths of
+    its centre (where it is above e^-40 of its peak)."""
     rng = np.random.default_rng(seed)
     d = len(N)
-    grids = np.meshgrid(*[np.arange(n, dtype=np.float64) for n in N], indexing="ij")
-    x = np.stack(grids, -1)
     radii = [0.0] + level_annuli(N, nbl, len(nbl))
     p0 = np.zeros(N)
     Nm = min(N)
+
+    def local_coords(sl):
+        ax = [np.arange(s.start, s.stop, dtype=np.float64) for s in sl]
+        return np.stack(np.meshgrid(*ax, indexing="ij"), -1)
+
     for i in range(n_packets):
         lvl = i % len(nbl)
         kmag = rng.uniform(max(radii[lvl], 1.0), radii[lvl + 1])
@@ -74,13 +86,17 @@ def make_p0(N, nbl, n_packets, n_blobs, blob_sigma, seed):
         c = (0.1 + 0.8 * rng.uniform(size=d)) * np.asarray(N)
         band = max(radii[lvl + 1] - radii[lvl], 1.0)
         width = Nm / (np.pi * band)
-        r = x - c
+        amp = rng.standard_normal()
+        sl = _window(N, c, 9.0 * width)
+        r = local_coords(sl) - c
         env = np.exp(-np.sum(r * r, -1) / (2 * width ** 2))
-        p0 += rng.standard_normal() * env * np.cos(2 * np.pi * kmag / Nm * (r @ u))
+        p0[sl] += amp * env * np.cos(2 * np.pi * kmag / Nm * (r @ u))
     for _ in range(n_blobs):
         c = (0.1 + 0.8 * rng.uniform(size=d)) * np.asarray(N)
-        r = x - c
-        p0 += rng.standard_normal() * np.exp(-np.sum(r * r, -1) / (2 * blob_sigma ** 2))
+        amp = rng.standard_normal()
+        sl = _window(N, c, 9.0 * blob_sigma)
+        r = local_coords(sl) - c
+        p0[sl] += amp * np.exp(-np.sum(r * r, -1) / (2 * blob_sigma ** 2))
     return p0 / np.max(np.abs(p0))
 
 
@@ -141,8 +157,28 @@ def config3(seed=0, thr=262144):
                          f"(4,8,16,32), four-sided sensor, thr={thr}, adaptive ODE")
 
 
-WORKLOADS = {"c2": config2, "het512": het512, "c3": config3}
-DEFAULT_THR = {"c2": 65536, "het512": 65536, "c3": 262144}
+def config5(seed=0, thr=262144):
+    """3D 128^3, dx 1e-4, c = 1500 (1 + 0.05 g) with a 20-cell correlation
+    length, 3 levels (4, 8, 16) per axis, 512 packets + 16 blobs (sigma 6
+    cells), planar sensor on the z = 0 face (128 x 128)."""
+    import beamax_b200 as bb
+
+    N, dx = (128, 128, 128), (1e-4, 1e-4, 1e-4)
+    c = random_speed(N, dx, 0.05, 20.0, seed + 17)
+    dom = bb.Domain(N=N, dx=dx, periodic=(False, False, False), cfl=0.3, c=c)
+    wpt = bb.MSWPT(bb.DyadicDecomposition(3, N, (4, 8, 16), (1, 1, 1)), 2, "rectangular_mirror")
+    mask = np.zeros(N)
+    mask[:, :, 0] = 1
+    sensors = bb.Sensor(dom, binary_mask=mask)
+    ts = dom.generate_time_domain()
+    p0 = make_p0(N, (4, 8, 16), 512, 16, 6.0, seed)
+    return dict(name=f"config5: 3D 128^3, c = 1500 (1 + 0.05 g), 20-cell correlation, 3 levels (4,8,16), "
+                     f"planar z=0 sensor 128x128, thr={thr}, adaptive ODE",
+                domain=dom, wpt=wpt, sensors=sensors, ts=ts, p0=p0, thr=thr, hetero=True)
+
+
+WORKLOADS = {"c2": config2, "het512": het512, "c3": config3, "c5": config5}
+DEFAULT_THR = {"c2": 65536, "het512": 65536, "c3": 262144, "c5": 262144}
 
 
 # ---------------------------------------------------------------- clocks
@@ -369,7 +405,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cutoff", type=float, default=16.0)
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2",
-                    help="c2: config 2 (the headline); het512 / c3: heterogeneous media")
+                    help="c2: config 2 (the headline); het512 / c3 / c5: heterogeneous media")
     ap.add_argument("--thr", type=int, default=None, help="top_n (default: the workload's; smaller for profiling)")
     ap.add_argument("--cpu-sample", type=int, default=96)
     ap.add_argument("--no-fp64", action="store_true")

@@ -359,3 +359,56 @@ def test_adjoint_reuses_forward_trajectories():
         a_keep = keep.adjoint(data, dom, sens, ts, wpt)
         a_fresh = fresh.adjoint(data, dom, sens, ts, wpt)
         assert om.rel_l2(a_fresh, a_keep) < (1e-12 if precision == "fp64" else 1e-6)
+
+
+def _het3d_case(thr):
+    import beamax_b200 as bb
+
+    N, dx = (32, 32, 32), (1e-4, 1e-4, 1e-4)
+    c, interp = _random_medium(N, dx, 0.05, 4.0, 21)
+    dom = bb.Domain(N=N, dx=dx, periodic=(False, False, False), cfl=0.3, c=interp)
+    wpt = bb.MSWPT(bb.DyadicDecomposition(2, N, (4, 8), (1, 1, 1)), 2, "rectangular_mirror")
+    xg = np.stack(np.meshgrid(*[np.arange(n) for n in N], indexing="ij"), -1).astype(float)
+    p0 = np.exp(-np.sum((xg - 15.0) ** 2, -1) / 20.0) * np.cos(0.8 * xg[..., 2])
+    mask = np.zeros(N)
+    mask[:, :, 0] = 1  # planar sensor on the z = 0 face
+    sens = bb.Sensor(dom, binary_mask=mask)
+    ts = dom.generate_time_domain()[::2]
+    return dom, wpt, p0, sens, ts, c
+
+
+def test_heterogeneous_3d_forward_matches_oracle_and_fp32_and_dot_test():
+    """3D (the 128^3 configuration's geometry at 32^3): FP64 forward against the
+    oracle's Dormand-Prince trajectories summed by the oracle (1e-7 rel-L2),
+    FP32 against FP64 (1e-3), and the FP64 transpose's dot test (1e-10)."""
+    import beamax_b200 as bb
+    from beamax_b200.solvers.msgb_solver import Selection
+
+    dev = _dev()
+    dom, wpt, p0, sens, ts, c = _het3d_case(thr=4)
+    ode = bb.gb.gb_solvers.solve_ODE_base
+    s64 = bb.MSGBSolver(4, "top_n", 64, "spatial", ode, "scan_real")
+    s32 = bb.MSGBSolver(4, "top_n", 64, "spatial", ode, "scan_real", precision="fp32")
+    y64 = s64.forward(p0, dom, sens, ts, wpt)
+    bt = s64.beams(s64.last_selection, dom, wpt)
+    x0, p0s = bt.x0.cpu().numpy(), bt.p0.cpu().numpy()
+    al, a0, w = bt.alpha.cpu().numpy(), bt.a0.cpu().numpy(), bt.omega.cpu().numpy()
+    speed = oo.GridSpeed(c, dom.dx, method="bspline3", boundary="clamp")
+    ref = np.zeros_like(y64)
+    for j in range(x0.shape[0]):
+        for mode in (1.0, -1.0):
+            xt, pt, Mt, At, st, _ = oo.dopri5(x0[j], p0s[j], np.diag(al[j]), a0[j], mode, ts, speed)
+            assert st == 0
+            ref += oo.beam_field(xt, pt, Mt, At, w[j], sens.positions, dom.grid_size, dom.periodic)
+    assert om.rel_l2(ref, y64) < 1e-7
+    y32 = s32.forward(p0, dom, sens, ts, wpt)
+    assert om.rel_l2(y64, y32) < 1e-3
+    sel = s64.last_selection
+    data = np.random.default_rng(6).standard_normal(y64.shape)
+    a64 = s64.adjoint(data, dom, sens, ts, wpt, selection=sel)
+    q = np.random.default_rng(7).standard_normal(dom.N)
+    cq = wpt.forward_device(torch.from_numpy(q).to(dev), scale=0.5, half_mask=True)
+    Aq = s64.sum_forward(s64.beams(Selection(sel.idx, cq[sel.idx], sel.total_coeffs), dom, wpt), dom, sens,
+                         ts).cpu().numpy()
+    lhs, rhs = float(np.sum(Aq * data)), float(np.sum(q * a64))
+    assert abs(lhs - rhs) <= 1e-10 * abs(lhs)
