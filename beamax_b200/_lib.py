@@ -86,6 +86,15 @@ class BeamOut(ctypes.Structure):
                 ("a0_unit", c_vp)]
 
 
+class TrGeometry(ctypes.Structure):
+    _fields_ = [("normal_axis", c_i32), ("normal_value", c_dbl), ("inward", c_dbl)]
+
+
+class TrBeams(ctypes.Structure):
+    _fields_ = [("n", c_i64), ("x", c_vp), ("p", c_vp), ("M", c_vp), ("a", c_vp), ("omega", c_vp),
+                ("mode", c_vp), ("t0", c_vp)]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "msgb_last_error": (ctypes.c_char_p, []),
@@ -128,6 +137,12 @@ SIGNATURES = {
     "msgb_topn_workspace_size": (c_sz, [c_i64, c_i64]),
     "msgb_topn": (ctypes.c_int, [c_vp, c_vp, c_i64, c_i64, c_vp, c_vp, c_vp, c_sz, c_vp]),
     "msgb_beam_init": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_i64, c_vp, c_vp]),
+    "msgb_tr_init": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_i64, ctypes.c_int, c_dbl, c_vp, c_vp]),
+    "msgb_adjoint_source_workspace_size": (c_sz, [c_i64, c_i64]),
+    "msgb_adjoint_source": (ctypes.c_int, [c_vp, c_vp, ctypes.c_int, c_i64, c_i64, c_dbl, c_vp, c_vp, c_vp, c_sz,
+                                           c_vp]),
+    "msgb_medium_speed": (ctypes.c_int, [c_i32, c_vp, c_vp, c_i64, c_vp, c_vp]),
+    "msgb_tr_final_states": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "msgb_scatter_coeff_grad": (ctypes.c_int, [c_vp, c_vp, c_i64, c_dbl, c_vp, ctypes.c_int,
                                                 c_vp, c_vp]),
 }

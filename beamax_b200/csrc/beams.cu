@@ -192,6 +192,160 @@ __global__ void dpdt_kernel(DpdtArgs A) {
     if (A.keys) A.keys[f] = sqrt(__dadd_rn(__dmul_rn(re, re), __dmul_rn(im, im)));
 }
 
+// compute_TR_parameters (tr_solver_utils.py:205-440) for one selected
+// coefficient of the boundary-data transform.
+struct TrInitArgs {
+    PlanView v;
+    double L[3];
+    msgb_tr_geometry geo;
+    MediumArgs med;
+    const int64_t *idx;
+    const double2 *values;
+    int64_t n;
+    int b_inverse;
+    double guard;
+    msgb_tr_beams out;
+};
+
+template <int D>
+__global__ void tr_init_kernel(TrInitArgs A) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    const PlanView &v = A.v;
+    const double pi = 3.141592653589793;
+    const int64_t flat = A.idx[i];
+    int l = 0;
+    while (l < v.levels - 1 && flat >= v.ccum[l + 1]) ++l;
+    const int64_t local = flat - v.ccum[l];
+    int S[3] = {1, 1, 1};
+    int64_t P = 1;
+    for (int a = 0; a < D; ++a) {
+        S[a] = 2 * v.bshape[l][a];
+        P *= S[a];
+    }
+    const int64_t box_local = local / P;
+    int64_t rem = local - box_local * P;
+    int k[3] = {0, 0, 0};
+    for (int a = D - 1; a >= 0; --a) {
+        k[a] = (int)(rem % S[a]);
+        rem /= S[a];
+    }
+    const int64_t box = v.bcum[l] + box_local;
+    double ch[D], Lls[D], sig[D], ats = 1.0, cycles = 0.0;
+    for (int a = 0; a < D; ++a) {
+        const int ci = v.centres[box * D + a];
+        ch[a] = (double)ci / A.L[a];
+        const double bl = (double)v.bl[l] / A.L[a] * (double)v.aspect[a];
+        Lls[a] = bl * v.red;
+        sig[a] = bl / 2.0;
+        ats *= sqrt((pi * A.L[a]) / (Lls[a] * (double)v.N[a])) * sig[a];
+        const int support = v.bl[l] * v.red * v.aspect[a];
+        const int half = support / 2;
+        const int parity = floordiv(ci + v.N[a] / 2, half);
+        const int sgn = 1 - 2 * (parity & 1);
+        const int rolls = sgn * (half / 2);
+        cycles += (double)(ci - rolls) * (double)k[a] / (double)support;
+    }
+    cycles = cycles - floor(cycles);
+    double ps, pc;
+    sincospi(2.0 * cycles, &ps, &pc);
+    const double tau = ch[0];
+    const double signum = tau > 0.0 ? -1.0 : (tau < 0.0 ? 1.0 : 0.0);
+    const double omega = fmax(fabs(tau), 1e-6);
+    const double t0 = (double)k[0] / Lls[0];
+    // position on the detector: normal axis fixed, tangential axes in order
+    const int na = A.geo.normal_axis;
+    double x[D];
+    int j = 0;
+    for (int a = 0; a < D; ++a) {
+        if (a == na) {
+            x[a] = A.geo.normal_value;
+        } else {
+            x[a] = (double)k[1 + j] / Lls[1 + j];
+            ++j;
+        }
+    }
+    double c, g[D], H[D * D];
+    speed_eval<D>(A.med, x, c, g, H);
+    double pu[D];
+    if (D == 1) {
+        const double nrm = fabs(ch[0]);
+        const double r = fmax((ch[0] / nrm / c) * (ch[0] / nrm / c), 0.0);
+        pu[0] = A.geo.inward * sqrt(r);
+    } else {
+        const double ta = fmax(fabs(tau), 1e-6);
+        double t2 = 0.0;
+        j = 0;
+        for (int a = 0; a < D; ++a)
+            if (a != na) {
+                pu[a] = c * ch[1 + j] / ta;
+                t2 += pu[a] * pu[a];
+                ++j;
+            }
+        pu[na] = A.geo.inward * sqrt(fmax(1.0 - t2, 0.0));
+    }
+    double p[D];
+    for (int a = 0; a < D; ++a) p[a] = 2.0 * pi * pu[a] / (D == 1 ? 1.0 : c);
+    // spatial Hessian from the spacetime one (mT_inverse, tr_solver_utils.py:116-170)
+    cd M[D][D];
+    double np2 = 0.0;
+    for (int a = 0; a < D; ++a) np2 += p[a] * p[a];
+    const double npn = sqrt(np2);
+    double xd[D], pd[D];
+    for (int a = 0; a < D; ++a) {
+        xd[a] = signum * c * p[a] / npn;
+        pd[a] = -signum * g[a] * npn;
+    }
+    cd alpha[D];
+    for (int a = 0; a < D; ++a) alpha[a] = cd{0.0, 2.0 * (pi * sig[a]) * (pi * sig[a]) / omega};
+    cd num = alpha[0] + cd{pd[0] * xd[0], 0.0};
+    for (int b = 1; b < D; ++b) {
+        num = num + cd{-pd[b] * xd[b], 0.0} + (xd[b] * xd[b]) * alpha[b];
+        const cd ur = cd{pd[b] / xd[0], 0.0} - (xd[b] / xd[0]) * alpha[b];
+        M[0][b] = ur;
+        M[b][0] = ur;
+        for (int m = 1; m < D; ++m) M[b][m] = m == b ? alpha[b] : cd{0.0, 0.0};
+    }
+    M[0][0] = (1.0 / (xd[0] * xd[0])) * num;
+    cd a = cd{ats * pc, ats * ps};
+    bool placeholder = p[na] == 0.0;  // grazing: zero contribution, numerically safe values
+    if (placeholder) a = cd{0.0, 0.0};
+    if (A.b_inverse) {
+        // -principal_b_inverse: i sign(W) / (2 c G), W = 2 pi tau,
+        // G = sqrt(W^2 - c^2 |2 pi k_tan|^2); zero (and placeholders) when
+        // evanescent, at W = 0 or within the relative guard of grazing.
+        const double W = 2.0 * pi * tau;
+        double q2 = 0.0;
+        for (int b2 = 1; b2 < D; ++b2) q2 += (2.0 * pi * ch[b2]) * (2.0 * pi * ch[b2]);
+        const double rad = W * W - (c * c) * q2;
+        const double G = sqrt(fmax(rad, 0.0));
+        const bool valid = rad > 0.0 && fabs(W) > 0.0 && G > A.guard * fabs(W);
+        const double sw = W > 0.0 ? 1.0 : -1.0;
+        a = valid ? a * cd{0.0, sw / (2.0 * c * G)} : cd{0.0, 0.0};
+        placeholder |= !valid;
+    }
+    a = a * cd{A.values[i].x, A.values[i].y};
+    if (placeholder) {
+        for (int b2 = 0; b2 < D; ++b2) {
+            p[b2] = 1.0;
+            for (int m = 0; m < D; ++m) M[b2][m] = m == b2 ? cd{0.0, 1.0} : cd{0.0, 0.0};
+        }
+    }
+    for (int b2 = 0; b2 < D; ++b2) {
+        A.out.x[i * D + b2] = x[b2];
+        A.out.p[i * D + b2] = p[b2];
+        for (int m = 0; m < D; ++m) {
+            A.out.M[2 * ((i * D + b2) * D + m)] = M[b2][m].re;
+            A.out.M[2 * ((i * D + b2) * D + m) + 1] = M[b2][m].im;
+        }
+    }
+    A.out.a[2 * i] = a.re;
+    A.out.a[2 * i + 1] = a.im;
+    A.out.omega[i] = omega;
+    A.out.mode[i] = signum;
+    A.out.t0[i] = t0;
+}
+
 struct ScatterArgs {
     const int64_t *idx;
     const double2 *g;
@@ -320,6 +474,44 @@ extern "C" int msgb_coefficients_dpdt(const msgb_mswpt *plan, const double *L, c
         default: dpdt_kernel<3><<<grid, blk, 0, st>>>(A); break;
     }
     return check_launch("msgb_coefficients_dpdt");
+}
+
+extern "C" int msgb_tr_init(const msgb_mswpt *data_plan, const double *data_L, const msgb_tr_geometry *geo,
+                            const msgb_medium *med, const int64_t *idx, const double *values, int64_t n,
+                            int b_inverse, double relative_guard, const msgb_tr_beams *out,
+                            msgb_stream_t stream) {
+    if (!data_plan || !data_L || !geo || !med || !out) return fail(MSGB_ERR_ARG, "msgb_tr_init: NULL argument");
+    if (n < 0) return fail(MSGB_ERR_ARG, "negative beam count");
+    if (n == 0) return MSGB_OK;
+    if (!idx || !values || !out->x || !out->p || !out->M || !out->a || !out->omega || !out->mode || !out->t0)
+        return fail(MSGB_ERR_ARG, "msgb_tr_init: NULL array");
+    TrInitArgs A{};
+    if (int e = plan_view(data_plan, A.v)) return e;
+    const int d = A.v.nd;
+    if (geo->normal_axis < 0 || geo->normal_axis >= d) return fail(MSGB_ERR_ARG, "normal axis out of range");
+    if (geo->inward != 1.0 && geo->inward != -1.0) return fail(MSGB_ERR_ARG, "inward must be +1 or -1");
+    for (int a = 0; a < 3; ++a) A.L[a] = a < d ? data_L[a] : 1.0;
+    A.geo = *geo;
+    msgb_problem pr{};
+    pr.ndim = d;
+    if (int e = medium_args(&pr, med, A.med)) return e;
+    A.idx = idx;
+    A.values = (const double2 *)values;
+    A.n = n;
+    if (b_inverse && !(relative_guard >= 0.0 && relative_guard < 1.0))
+        return fail(MSGB_ERR_ARG, "relative_guard must lie in [0, 1)");
+    A.b_inverse = b_inverse != 0;
+    A.guard = relative_guard;
+    A.out = *out;
+    const int blk = 128;
+    const unsigned grid = (unsigned)((n + blk - 1) / blk);
+    cudaStream_t st = as_stream(stream);
+    switch (d) {
+        case 1: tr_init_kernel<1><<<grid, blk, 0, st>>>(A); break;
+        case 2: tr_init_kernel<2><<<grid, blk, 0, st>>>(A); break;
+        default: tr_init_kernel<3><<<grid, blk, 0, st>>>(A); break;
+    }
+    return check_launch("msgb_tr_init");
 }
 
 extern "C" int msgb_scatter_coeff_grad(const int64_t *idx, const double *g, int64_t n, double scale,

@@ -399,10 +399,97 @@ __global__ void rk4_kernel(ProbArgs P, MediumArgs med, BeamArgs B, TrajArgs T, O
     if (T.status) T.status[bl] = code;
 }
 
+// Time reversal: beam i starts on the detector at t0[i] and runs back to
+// t = 0.  With tau = t0 - t the state obeys dy/dtau = -f(y; mode, lam) =
+// f(y; -mode, -lam) (every term of the right-hand side is odd in the branch
+// except lam G / 2G), so the forward integrator runs unchanged over
+// tau in [0, t0] on the flipped branch and absorption.
+struct TrBeamsView {
+    const double *x, *p, *M, *mode, *t0;
+};
+
+template <int D>
+__global__ void tr_final_kernel(ProbArgs P, MediumArgs med, TrBeamsView B, int64_t n, OdeArgs o, double *rec64,
+                                int32_t *status) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    DopriBeam<D> s;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        s.y.x[a] = B.x[i * D + a];
+        s.y.p[a] = B.p[i * D + a];
+#pragma unroll
+        for (int b = 0; b < D; ++b)
+            s.y.M[a][b] = cd{B.M[2 * ((i * D + a) * D + b)], B.M[2 * ((i * D + a) * D + b) + 1]};
+    }
+    s.y.A = cd{1.0, 0.0};
+    const double t0 = B.t0[i];
+    int code = 0;
+    if (t0 > 0.0) {
+        double tl[2] = {0.0, t0};
+        ProbArgs Pl = P;
+        Pl.nt = 2;
+        Pl.ts = tl;
+        TrajArgs T{n, 0, n, nullptr, nullptr, nullptr, nullptr};  // records written below
+        RecordWriter<D> rw(Pl, T, i, 1.0, 2);
+        s.init(med, Pl, o, -B.mode[i]);
+        while (!s.attempt(med, Pl, o, rw)) {
+        }
+        code = s.code;
+    }
+    bool fin = isfinite(s.y.A.re) && isfinite(s.y.A.im);
+#pragma unroll
+    for (int a = 0; a < D; ++a) fin = fin && isfinite(s.y.x[a]) && isfinite(s.y.p[a]);
+    if (!fin && code == 0) code = 1;
+    double *r = rec64 + i * (int64_t)NV<D>::value;
+    const double *v = vals(s.y);
+#pragma unroll
+    for (int c = 0; c < NV<D>::value; ++c) r[c] = v[c];
+    status[i] = code;
+}
+
 }  // namespace
 }  // namespace msgb
 
 using namespace msgb;
+
+extern "C" int msgb_tr_final_states(const msgb_problem *prob, const msgb_medium *med, const msgb_tr_beams *beams,
+                                    const msgb_ode_opts *opts, double *rec64, int32_t *status,
+                                    msgb_stream_t stream) {
+    if (!prob || !med || !beams || !opts) return fail(MSGB_ERR_ARG, "msgb_tr_final_states: NULL argument");
+    if (prob->ndim < 1 || prob->ndim > 3) return fail(MSGB_ERR_ARG, "ndim must be 1, 2 or 3");
+    if (beams->n < 0) return fail(MSGB_ERR_ARG, "negative beam count");
+    if (opts->method != MSGB_ODE_DOPRI5) return fail(MSGB_ERR_ARG, "time reversal integrates with DOPRI5");
+    if (!(opts->rtol > 0.0) || !(opts->atol > 0.0) || !isfinite(opts->rtol) || !isfinite(opts->atol))
+        return fail(MSGB_ERR_ARG, "rtol and atol must be finite and positive");
+    if (opts->max_steps < 1) return fail(MSGB_ERR_ARG, "max_steps must be a positive integer");
+    if (!isfinite(opts->dt0)) return fail(MSGB_ERR_ARG, "dt0 must be finite");
+    if (beams->n == 0) return MSGB_OK;
+    if (!beams->x || !beams->p || !beams->M || !beams->mode || !beams->t0 || !rec64 || !status)
+        return fail(MSGB_ERR_ARG, "msgb_tr_final_states: NULL array");
+    MediumArgs M;
+    if (int e = medium_args(prob, med, M)) return e;
+    M.lam = -M.lam;
+    ProbArgs P{};
+    P.nd = prob->ndim;
+    for (int a = 0; a < 3; ++a) {
+        P.periodic[a] = a < prob->ndim ? (prob->periodic[a] != 0) : 0;
+        P.L[a] = a < prob->ndim ? prob->L[a] : 1.0;
+    }
+    P.c = prob->c;
+    OdeArgs O{opts->method, opts->substeps, opts->rtol, opts->atol, opts->dt0, opts->max_steps, 0,
+              opts->dense_output};
+    TrBeamsView B{beams->x, beams->p, beams->M, beams->mode, beams->t0};
+    const int blk = 64;
+    const unsigned grid = (unsigned)((beams->n + blk - 1) / blk);
+    cudaStream_t st = as_stream(stream);
+    switch (prob->ndim) {
+        case 1: tr_final_kernel<1><<<grid, blk, 0, st>>>(P, M, B, beams->n, O, rec64, status); break;
+        case 2: tr_final_kernel<2><<<grid, blk, 0, st>>>(P, M, B, beams->n, O, rec64, status); break;
+        default: tr_final_kernel<3><<<grid, blk, 0, st>>>(P, M, B, beams->n, O, rec64, status); break;
+    }
+    return check_launch("msgb_tr_final_states");
+}
 
 extern "C" int msgb_ode_trajectories(const msgb_problem *prob, const msgb_medium *med, const msgb_beam_set *beams,
                                      const msgb_ode_opts *opts, const msgb_trajectories *out,

@@ -17,8 +17,10 @@ map with the beam selection frozen (the reference's jax.vjp pattern,
 examples/diagnostics/msgb_adjoint_pairing.py:156-165): per-beam gathers
 (``msgb_adj_gather_*``), a scatter to coefficient space and the Hermitian
 adjoint of the MSWPT.  The reference's own principal-symbol ``adjoint`` (seven
-arguments, msgb_solver.py:1235-1386) is a different operator and raises
-``NotImplementedError`` here.
+arguments, msgb_solver.py:1235-1386) is a different operator; called with
+those arguments, ``adjoint`` computes it, and ``time_reversal`` the time
+reversal (:984-1111), both from boundary data with ``msgb_tr_init`` and
+``msgb_tr_final_states``.
 """
 
 from __future__ import annotations
@@ -773,22 +775,25 @@ class MSGBSolver:
             params = [p.cpu().numpy() for p in params]
         return tuple(params)
 
-    def adjoint(self, data, domain: Domain, sensors, ts, wpt: MSWPT, *args, p0=None,
-                selection: Optional[Selection] = None, **kwargs):
-        """Exact transpose A^T d of ``forward`` with the beam selection frozen.
+    def adjoint(self, data, domain: Domain, sensors, *args, **kwargs):
+        """Two operators, told apart by their arguments:
 
-        The selection is ``selection`` if given, else the one made from ``p0``,
-        else the one made by this solver's last ``forward``.  Returns the image
-        (shape domain.N), float64.  The reference's seven-argument
-        principal-symbol adjoint is not this operator.
+        * ``adjoint(data, domain, sensors, ts, wpt, *, p0=None, selection=None)``:
+          the exact transpose A^T d of ``forward`` with the beam selection
+          frozen (the selection is ``selection`` if given, else the one made
+          from ``p0``, else the one of this solver's last ``forward``); returns
+          the image (shape domain.N), float64.
+        * ``adjoint(data, domain, sensors, sources, ts, data_domain, data_wpt,
+          *, window=None)``: the reference's principal-symbol approximation of
+          the continuous PAT adjoint (msgb_solver.py:1235-1386), evaluated at
+          the sensor positions; not the transpose of the discrete forward.
         """
-        if args or {"sources", "data_domain", "data_wpt", "window"} & set(kwargs):
-            raise NotImplementedError(
-                "the principal-symbol adjoint adjoint(data, domain, sensors, sources, ts, data_domain, "
-                "data_wpt) is not implemented; adjoint(data, domain, sensors, ts, wpt) is the exact "
-                "transpose of forward")
-        if kwargs:
-            raise TypeError(f"unexpected keyword arguments {sorted(kwargs)}")
+        if len(args) > 2 or {"sources", "data_domain", "data_wpt", "window"} & set(kwargs):
+            return self.adjoint_with_params(data, domain, sensors, *args, **kwargs)[0]
+        return self._exact_adjoint(data, domain, sensors, *args, **kwargs)
+
+    def _exact_adjoint(self, data, domain: Domain, sensors, ts, wpt: MSWPT, *, p0=None,
+                       selection: Optional[Selection] = None):
         if wpt.dyadic_decomp.N != domain.N:
             raise ValueError("wpt grid shape must match domain.N.")
         _validate_time_grid(ts, allow_singleton=True)
@@ -853,6 +858,244 @@ class MSGBSolver:
                                                           torch.view_as_real(G).data_ptr(), st),
                        "msgb_scatter_coeff_grad")
         return wpt.adjoint(G, "spatial", real_output=False)
+
+    # ------------------------------------------------------------- time reversal
+    def _validate_boundary_data(self, data, data_domain: Domain, sources, *, ts=None) -> None:
+        """msgb_solver.py:806-856: the regular axis-aligned detector grid."""
+        shape = tuple(data.shape)
+        if shape != tuple(data_domain.N):
+            raise ValueError(f"Boundary data must have shape {tuple(data_domain.N)}; got {shape}.")
+        if ts is not None:
+            _validate_time_grid(ts)
+            ts_np = np.asarray(ts.detach().cpu().numpy() if hasattr(ts, "detach") else ts, np.float64)
+            data_span = (shape[0] - 1) * data_domain.dx[0]
+            acquisition_span = float(ts_np[-1] - ts_np[0])
+            if not np.isclose(acquisition_span, data_span, rtol=1e-6, atol=1e-12):
+                raise ValueError(f"ts spans {acquisition_span}, but data_domain spans {data_span}.")
+        if not isinstance(sources, Sensor):
+            raise ValueError("sources must be a Sensor on a regular planar grid.")
+        positions = np.asarray(sources.positions, np.float64)
+        stds = np.std(positions, axis=0)
+        normal_axis = int(np.argmin(stds))
+        tolerance = 1e-7 * max(1.0, float(np.max(sources.domain.grid_size)))
+        if stds[normal_axis] > tolerance:
+            raise ValueError("sources must lie on an axis-aligned planar surface.")
+        counts = []
+        for axis in (a for a in range(positions.shape[1]) if a != normal_axis):
+            values = np.unique(positions[:, axis])
+            if values.size > 2 and not np.allclose(np.diff(values), np.diff(values)[0], rtol=1e-6, atol=tolerance):
+                raise ValueError("sources must be uniformly spaced on the detector plane.")
+            counts.append(int(values.size))
+        expected = tuple(counts) if counts else (1,)
+        actual = tuple(shape[1:]) or (1,)
+        if actual != expected:
+            raise ValueError("Boundary data detector axes do not match the source grid: "
+                             f"got {actual}, expected {expected}.")
+        if math.prod(expected) != positions.shape[0]:
+            raise ValueError("sources must form a complete Cartesian detector grid.")
+
+    @staticmethod
+    def _tr_geometry(sources: Sensor) -> _lib.TrGeometry:
+        """The detector plane (tr_solver_utils.py:173-204, 241-251, 377-393):
+        the first constant column of the source positions is the normal axis
+        (axis 0 at value 0 when none is), and the normal momentum points into
+        the domain."""
+        pos = np.asarray(sources.positions, np.float64)
+        const = np.nonzero(np.all(pos == pos[0], axis=0))[0]
+        axis = int(const[0]) if const.size else 0
+        value = float(pos[0, axis]) if const.size else 0.0
+        dx = np.asarray(sources.domain.dx, np.float64)
+        grid_max = float(np.asarray(sources.domain.grid_size, np.float64)[axis] - dx[axis])
+        if np.isclose(value, 0.0):
+            inward = 1.0
+        elif np.isclose(value, grid_max):
+            inward = -1.0
+        else:
+            inward = float(np.sign(grid_max / 2.0 - value)) or 1.0
+        return _lib.TrGeometry(normal_axis=axis, normal_value=value, inward=inward)
+
+    def time_reversal(self, data, domain: Domain, sensors, sources, ts, data_domain: Domain, data_wpt: MSWPT):
+        """MSGB time-reversal reconstruction at the positions of ``sensors``
+        (msgb_solver.py:984-1041), scaled by 2."""
+        return self.time_reversal_with_params(data, domain, sensors, sources, ts, data_domain, data_wpt)[0]
+
+    def time_reversal_with_params(self, data, domain: Domain, sensors, sources, ts, data_domain: Domain,
+                                  data_wpt: MSWPT):
+        """msgb_solver.py:1043-1111 on the GPU: c_pos = 0.5 MSWPT_data(data)
+        (no half-frame mask), the solver's threshold, msgb_tr_init (beams on
+        the detector at their data time), msgb_tr_final_states (each beam
+        back to t = 0, adaptive FP64 with the solver's tolerances), the FP64
+        trajectory sum at the sensor positions, times 2.  Returns the image
+        (Ns,) and the beam parameters (pts, Mts, xts, omegas, ats, signum, ts)
+        with ts (n, 2) = (start, 0) as compute_TR_parameters returns them."""
+        if any(domain.periodic):
+            raise ValueError("The MSGB time reversal solver only supports free space boundary conditions.")
+        pos = self._sensor_positions(sensors)
+        self._validate_boundary_data(data, data_domain, sources, ts=ts)
+        self._check_tr_axes(domain, sources, data_domain)
+        x = as_device_f64(data)
+        if x.is_complex():
+            raise ValueError("time reversal takes real boundary data")
+        coeffs, keys = data_wpt.forward_device(x, self.input_type, scale=0.5, keys=True)
+        sel = self._select_from(coeffs, keys, data_wpt, x.device, self._effective_top_n(data_wpt))
+        out, params = self._boundary_beams_to_image(sel, domain, pos, sources, data_domain, data_wpt,
+                                                    b_inverse=False)
+        return self._tr_output(2.0 * out, params, data)
+
+    def adjoint_with_params(self, data, domain: Domain, sensors, sources, ts, data_domain: Domain,
+                            data_wpt: MSWPT, *, window=None):
+        """The principal-symbol adjoint (msgb_solver.py:1235-1386) on the GPU:
+        F = -c_Gamma^2 d_t(window r) (msgb_adjoint_source), raw MSWPT_data(F)
+        coefficients, the solver's threshold (uncapped top_n), the time
+        reversal beams with amplitudes times -B^{-1} (msgb_tr_init with
+        b_inverse, relative guard ``adjoint_relative_guard``), each back to
+        t = 0, the FP64 field at the sensor positions divided by c^2 there.
+        Returns (q_T (Ns,), beam parameters)."""
+        import torch
+
+        if any(domain.periodic):
+            raise ValueError("MSGBSolver.adjoint currently assumes non-periodic spatial "
+                             "boundaries in the reconstruction domain.")
+        try:
+            pos = self._sensor_positions(sensors)
+        except ValueError:
+            raise ValueError("Unsupported sensor type for `sensors` in adjoint().") from None
+        self._validate_boundary_data(data, data_domain, sources, ts=ts)
+        self._check_tr_axes(domain, sources, data_domain)
+        x = as_device_f64(data)
+        if x.is_complex():
+            raise ValueError("the principal-symbol adjoint takes real boundary data")
+        dev = x.device
+        nt = int(x.shape[0])
+        ns = int(np.prod(x.shape[1:])) if x.dim() > 1 else 1
+        src_pos = torch.from_numpy(np.ascontiguousarray(sources.positions, np.float64)).to(dev)
+        if src_pos.shape[0] != ns:
+            raise ValueError(f"c_at_sources has {src_pos.shape[0]} detector samples, which does not match "
+                             f"the data detector grid {tuple(x.shape[1:])}.")
+        c_src = self._speed_at(sources.domain, src_pos)
+        w = None
+        w_time = 0
+        if window is not None:
+            w = as_device_f64(window, dev)
+            if w.dim() == 1 and x.dim() > 1:
+                if w.shape[0] != nt:
+                    raise ValueError(f"a time window needs {nt} samples; got {w.shape[0]}")
+                w_time = 1
+            elif tuple(w.shape) != tuple(x.shape):
+                raise ValueError(f"window must have shape {tuple(x.shape)} or ({nt},); got {tuple(w.shape)}")
+            w = w.contiguous()
+        src = torch.empty_like(x)
+        nbytes = _lib.lib().msgb_adjoint_source_workspace_size(nt, ns)
+        if nbytes == 0:
+            raise RuntimeError("msgb_adjoint_source_workspace_size: " + _lib.last_error())
+        ws = workspace(dev, "adjsrc", nbytes)
+        st = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(_lib.lib().msgb_adjoint_source(x.contiguous().data_ptr(), None if w is None else w.data_ptr(),
+                                                  w_time, nt, ns, float(data_domain.dx[0]), c_src.data_ptr(),
+                                                  src.data_ptr(), ws.data_ptr(), nbytes, st), "msgb_adjoint_source")
+        coeffs, keys = data_wpt.forward_device(src, self.input_type, scale=1.0, keys=True)
+        sel = self._select_from(coeffs, keys, data_wpt, dev, self._effective_top_n(data_wpt))
+        out, params = self._boundary_beams_to_image(sel, domain, pos, sources, data_domain, data_wpt,
+                                                    b_inverse=True)
+        img_pos = torch.from_numpy(np.ascontiguousarray(pos, np.float64)).to(dev)
+        c_img = self._speed_at(domain, img_pos)
+        return self._tr_output(out / (c_img * c_img), params, data)
+
+    @staticmethod
+    def _check_tr_axes(domain: Domain, sources, data_domain: Domain):
+        if data_domain.ndim != domain.ndim or sources.domain.ndim != domain.ndim:
+            raise ValueError("data_domain, sources and domain must have the same number of axes")
+
+    def _speed_at(self, domain: Domain, points):
+        """c(x) of ``domain`` at device points (n, d) (msgb_medium_speed)."""
+        import torch
+
+        med, keep = self._medium(domain, points.device)
+        c = torch.empty(points.shape[0], dtype=torch.float64, device=points.device)
+        st = torch.cuda.current_stream(points.device).cuda_stream
+        _lib.check(_lib.lib().msgb_medium_speed(domain.ndim, _lib.ref(med), points.data_ptr(), int(points.shape[0]),
+                                                c.data_ptr(), st), "msgb_medium_speed")
+        del keep
+        return c
+
+    @staticmethod
+    def _tr_output(img, params, data):
+        if not _is_torch(data):
+            img = img.cpu().numpy()
+            params = tuple(p.cpu().numpy() for p in params)
+        return img, params
+
+    def _boundary_beams_to_image(self, sel: Selection, domain: Domain, pos, sources, data_domain: Domain,
+                                 data_wpt: MSWPT, b_inverse: bool):
+        """Beams from boundary-data coefficients (msgb_tr_init), each from its
+        data time back to t = 0 (msgb_tr_final_states), the FP64 real field
+        at ``pos`` (msgb_sum_fwd_f64_traj with nt = 1): compute_TR_result
+        (tr_solver_utils.py:677-750).  Returns the field (Ns,) and the
+        parameters (pts, Mts, xts, omegas, ats (n, 1), signum (n, 1), ts (n, 2))."""
+        import torch
+
+        dev = sel.idx.device
+        d = domain.ndim
+        n = int(sel.idx.shape[0])
+        self.last_boundary_selection = sel
+        xs = torch.empty((n, d), dtype=torch.float64, device=dev)
+        ps = torch.empty((n, d), dtype=torch.float64, device=dev)
+        Ms = torch.empty((n, d, d), dtype=torch.complex128, device=dev)
+        a = torch.empty(n, dtype=torch.complex128, device=dev)
+        om = torch.empty(n, dtype=torch.float64, device=dev)
+        mode = torch.empty(n, dtype=torch.float64, device=dev)
+        t0 = torch.empty(n, dtype=torch.float64, device=dev)
+        tb = _lib.TrBeams(n=n, x=xs.data_ptr(), p=ps.data_ptr(), M=torch.view_as_real(Ms).data_ptr(),
+                          a=torch.view_as_real(a).data_ptr(), omega=om.data_ptr(), mode=mode.data_ptr(),
+                          t0=t0.data_ptr())
+        geo = self._tr_geometry(sources)
+        src_med, keep_s = self._medium(sources.domain, dev)
+        Ld = (ctypes.c_double * 3)(*[float(v) for v in data_domain.grid_size], *([1.0] * (3 - d)))
+        st = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(_lib.lib().msgb_tr_init(data_wpt.plan(dev), Ld, _lib.ref(geo), _lib.ref(src_med),
+                                           sel.idx.data_ptr(), torch.view_as_real(sel.values).data_ptr(), n,
+                                           int(b_inverse), float(self.adjoint_relative_guard), _lib.ref(tb), st),
+                   "msgb_tr_init")
+        med, keep_m = self._medium(domain, dev)
+        cfg = self.ode_config
+        opts = _lib.OdeOpts(method=1, substeps=1, rtol=float(cfg.rtol), atol=float(cfg.atol),
+                            dt0=float(cfg.dt0) if cfg.dt0 is not None else 0.0, max_steps=int(cfg.max_steps),
+                            dense_output=int(bool(cfg.dense_output)))
+        sens = torch.from_numpy(np.ascontiguousarray(pos, np.float64)).to(dev)
+        t_img = torch.zeros(1, dtype=torch.float64, device=dev)
+        pr = _lib.Problem()
+        pr.ndim = d
+        L = np.asarray(domain.grid_size, np.float64)
+        for ax in range(3):
+            pr.periodic[ax] = 0
+            pr.L[ax] = float(L[ax]) if ax < d else 1.0
+        pr.c = 1.0
+        pr.nt = 1
+        pr.ts = t_img.data_ptr()
+        pr.ns = pos.shape[0]
+        pr.sensors = sens.data_ptr()
+        nr = 2 * d + 2 * d * d + 2
+        rec = torch.empty((n, nr), dtype=torch.float64, device=dev)
+        status = torch.zeros(n, dtype=torch.int32, device=dev)
+        out = torch.zeros((1, pos.shape[0]), dtype=torch.float64, device=dev)
+        if n:
+            with self._kernel_span("msgb_tr_final_states", None):
+                _lib.check(_lib.lib().msgb_tr_final_states(_lib.ref(pr), _lib.ref(med), _lib.ref(tb), _lib.ref(opts),
+                                                           rec.data_ptr(), status.data_ptr(), st),
+                           "msgb_tr_final_states")
+            worst = int(status.max().item())
+            if worst:
+                what = "reached max_steps" if worst == 2 else "produced a non-finite state"
+                raise RuntimeError(f"time-reversal ODE integration {what} for "
+                                   f"{int((status == worst).sum().item())} beam(s)")
+            bs = _lib.BeamSet(n=n, x0=xs.data_ptr(), p0=ps.data_ptr(), alpha=torch.view_as_real(Ms).data_ptr(),
+                              a0=torch.view_as_real(a).data_ptr(), omega=om.data_ptr(), modes=0)
+            tr = _lib.Trajectories(nb=n, b_first=0, rec64=rec.data_ptr(), rec32=None, cull=None, status=None)
+            _lib.check(_lib.lib().msgb_sum_fwd_f64_traj(_lib.ref(pr), _lib.ref(bs), _lib.ref(tr), out.data_ptr(), st),
+                       "msgb_sum_fwd_f64_traj")
+        del keep_s, keep_m
+        ts_pair = torch.stack([t0, torch.zeros_like(t0)], dim=1)
+        return out[0], (ps, Ms, xs, om, a[:, None], mode[:, None], ts_pair)
 
     def eval_count(self) -> Optional[int]:
         """Evaluated (beam, time, sensor) triples of the last FP32 call."""

@@ -440,6 +440,63 @@ int msgb_coefficients_dpdt(const msgb_mswpt *plan, const double *L, const msgb_m
                            const double *a, const double *b, int branch, int apply_half_mask,
                            double *out, double *keys, msgb_stream_t stream);
 
+/* ---- time reversal ------------------------------------------------------ */
+/* MSGBSolver.time_reversal (solvers/msgb_solvers/msgb_solver.py:984-1111):
+ * beams launched from a planar detector at their data time
+ * (tr_solver_utils.py:205-440), integrated back to t = 0 and summed at image
+ * points with msgb_sum_fwd_f64_traj (one time, rec64 of the final states,
+ * beam amplitudes a, frequencies omega). */
+typedef struct msgb_tr_geometry {
+    int32_t normal_axis;     /* spatial axis normal to the detector plane */
+    double normal_value;     /* the detector's coordinate on that axis */
+    double inward;           /* +1 or -1: sign of the normal momentum into the domain */
+} msgb_tr_geometry;
+
+typedef struct msgb_tr_beams {
+    int64_t n;
+    double *x, *p;           /* (n, d) position and momentum on the detector */
+    double *M;               /* (n, d, d) complex spatial Hessian */
+    double *a;               /* (n) complex amplitude, times the coefficient */
+    double *omega;           /* (n) frequency |tau| */
+    double *mode;            /* (n) branch -sign(tau) */
+    double *t0;              /* (n) launch time */
+} msgb_tr_beams;
+
+/* compute_TR_parameters (tr_solver_utils.py:205-440) for the selected
+ * data-transform coefficients (flat indices idx, values c[idx]): data_plan is
+ * the boundary-data MSWPT (axis 0 time, then the detector's tangential axes),
+ * data_L its physical lengths (host, ndim), med the medium at the detector.
+ * With b_inverse != 0, compute_adj_parameters (adjoint_solver_utils.py:
+ * 78-200) instead: the amplitude times -B^{-1}(tau, k_tan, c(x_T)) of
+ * principal_b_inverse (:17-75) with the given relative_guard, and beams whose
+ * multiplier is 0 get the grazing placeholders.  Writes every field of out. */
+int msgb_tr_init(const msgb_mswpt *data_plan, const double *data_L, const msgb_tr_geometry *geo,
+                 const msgb_medium *med, const int64_t *idx, const double *values, int64_t n,
+                 int b_inverse, double relative_guard, const msgb_tr_beams *out, msgb_stream_t stream);
+
+/* _form_adjoint_source (msgb_solver.py:68-120): out (nt, ns) = -c_s^2
+ * Re(ifft_t(2 pi i fftfreq(nt, dt) fft_t(window r))), r (nt, ns) row-major,
+ * window NULL, (nt) (window_is_time_only) or (nt, ns), c_at_sources (ns).
+ * Creates (and destroys) a batched cuFFT plan per call; the workspace holds
+ * the spectrum and cuFFT's work area. */
+size_t msgb_adjoint_source_workspace_size(int64_t nt, int64_t ns);
+int msgb_adjoint_source(const double *data, const double *window, int window_is_time_only, int64_t nt,
+                        int64_t ns, double dt, const double *c_at_sources, double *out, void *workspace,
+                        size_t workspace_bytes, msgb_stream_t stream);
+
+/* c(x) of the medium at n points x (n, ndim) (Domain.c_fn, geometry.py:
+ * 176-221, for the medium kinds of msgb_medium). */
+int msgb_medium_speed(int32_t ndim, const msgb_medium *med, const double *x, int64_t n, double *c,
+                      msgb_stream_t stream);
+
+/* Each beam integrated from its launch time back to t = 0 (adaptive FP64,
+ * opts as msgb_ode_trajectories; time reversed by flipping the branch and the
+ * absorption sign), amplitude from 1.  rec64: (n, 2d + 2d^2 + 2) final states;
+ * status (n): 0 ok, 1 non-finite, 2 step budget exhausted.  prob supplies
+ * ndim, L and periodic. */
+int msgb_tr_final_states(const msgb_problem *prob, const msgb_medium *med, const msgb_tr_beams *beams,
+                         const msgb_ode_opts *opts, double *rec64, int32_t *status, msgb_stream_t stream);
+
 /* ---- adjoint scatter to coefficient space ------------------------------ */
 
 /* G[idx[j]] += scale * g[j] for unique idx (no atomics needed); G must be

@@ -135,12 +135,22 @@ def test_domain_and_sensor_match_reference_conventions():
     assert bb.Domain(N=(4, 4), dx=(1.0, 1.0), periodic=(True, True), c=lambda x: 2.0 + 0 * x[..., 0]).constant_speed() == 2.0
 
 
-def test_adjoint_reference_signature_is_explicitly_not_this_operator():
-    w = bb.MSWPT(bb.DyadicDecomposition(1, (16,), (4,), (1,)), 2, "rectangular")
-    d = bb.Domain(N=(16,), dx=(1.0,), periodic=(False,))
-    s = bb.MSGBSolver(4, "top_n", 4, "spatial", "solve_hom_diag", "all_real")
-    with pytest.raises(NotImplementedError, match="principal-symbol"):
-        s.adjoint(np.zeros((3, 1)), d, np.zeros((1, 1)), object(), np.arange(3.0), d, w)
+def test_adjoint_seven_argument_form_is_the_principal_symbol_adjoint():
+    """adjoint(data, domain, sensors, sources, ts, data_domain, data_wpt) takes
+    the reference's principal-symbol path and its checks (msgb_solver.py:
+    1339-1356, 806-856), before any device work."""
+    s, dom, ts, ddom, wpt, src, data = _tr_case()
+    img = bb.Sensor(dom, binary_mask=np.ones(dom.N))
+    per = bb.Domain(N=dom.N, dx=dom.dx, periodic=(True, True), cfl=0.3, c=1500.0)
+    with pytest.raises(ValueError, match="non-periodic spatial boundaries"):
+        s.adjoint(data, per, img, src, ts, ddom, wpt)
+    with pytest.raises(ValueError, match="Unsupported sensor type for `sensors` in adjoint"):
+        s.adjoint(data, dom, object(), src, ts, ddom, wpt)
+    with pytest.raises(ValueError, match="Boundary data must have shape"):
+        s.adjoint(data=data[:, :-1], domain=dom, sensors=img, sources=src, ts=ts, data_domain=ddom,
+                  data_wpt=wpt, window=np.ones(data.shape[0]))
+    with pytest.raises(TypeError):
+        s.adjoint(data, dom, img, src, ts, ddom, wpt, p0=np.zeros(dom.N))
 
 
 def test_solver_config_matches_reference_checks():
@@ -168,3 +178,55 @@ def test_solver_config_matches_reference_checks():
     assert solver.ode_config == SolverConfig()
     with pytest.raises(TypeError):
         bb.MSGBSolver(8, "top_n", 8, "spatial", bb.gb.gb_solvers.solve_ODE_base, "scan_real", ode_config={})
+
+
+def _tr_case(N=(32, 32)):
+    dom = bb.Domain(N=N, dx=(1e-4,) * len(N), periodic=(False,) * len(N), cfl=0.3, c=1500.0)
+    ts = dom.generate_time_domain()
+    Nd = (2 * N[0],) + tuple(N[1:])
+    ddom = bb.Domain(N=Nd, dx=(float(ts[-1] / (Nd[0] - 1)),) + (1e-4,) * (len(N) - 1),
+                     periodic=(False,) * len(N), cfl=0.3, c=1500.0)
+    wpt = bb.MSWPT(bb.DyadicDecomposition(2, Nd, (4, 8), (2, 1)), 2, "rectangular_mirror")
+    mask = np.zeros(N)
+    mask[0, :] = 1
+    src = bb.Sensor(dom, binary_mask=mask)
+    s = bb.MSGBSolver(200, "top_n", 64, "spatial", bb.gb.gb_solvers.solve_ODE_base, "scan_real")
+    return s, dom, ts, ddom, wpt, src, np.zeros(Nd)
+
+
+def test_time_reversal_input_checks_match_reference():
+    """msgb_solver.py:1079-1082 and :806-856 (checked before any device work)."""
+    s, dom, ts, ddom, wpt, src, data = _tr_case()
+    img = bb.Sensor(dom, binary_mask=np.ones(dom.N))
+    per = bb.Domain(N=dom.N, dx=dom.dx, periodic=(True, True), cfl=0.3, c=1500.0)
+    with pytest.raises(ValueError, match="only supports free space boundary"):
+        s.time_reversal(data, per, img, src, ts, ddom, wpt)
+    with pytest.raises(ValueError, match="Boundary data must have shape"):
+        s.time_reversal(data[:-1], dom, img, src, ts, ddom, wpt)
+    with pytest.raises(ValueError, match="ts spans"):
+        s.time_reversal(data, dom, img, src, ts[:-5], ddom, wpt)
+    with pytest.raises(ValueError, match="sources must be a Sensor"):
+        s.time_reversal(data, dom, img, np.asarray(src.positions), ts, ddom, wpt)
+    tilted = bb.Sensor(dom, positions=np.stack([np.arange(32) * 1e-4, np.arange(32) * 1e-4], 1))
+    with pytest.raises(ValueError, match="axis-aligned planar surface"):
+        s.time_reversal(data, dom, img, tilted, ts, ddom, wpt)
+    half = bb.Sensor(dom, positions=np.stack([np.zeros(16), np.arange(16) * 1e-4], 1))
+    with pytest.raises(ValueError, match="detector axes do not match"):
+        s.time_reversal(data, dom, img, half, ts, ddom, wpt)
+
+
+def test_time_reversal_detector_geometry():
+    """Normal axis and inward sign of the detector (tr_solver_utils.py:241-251,
+    377-393): first row -> axis 0 inward +1, last row -> -1, first column ->
+    axis 1."""
+    s, dom, ts, ddom, wpt, src, data = _tr_case()
+    g = s._tr_geometry(src)
+    assert (g.normal_axis, g.normal_value, g.inward) == (0, 0.0, 1.0)
+    mask = np.zeros(dom.N)
+    mask[-1, :] = 1
+    g = s._tr_geometry(bb.Sensor(dom, binary_mask=mask))
+    assert (g.normal_axis, g.inward) == (0, -1.0) and g.normal_value == pytest.approx(31e-4)
+    mask = np.zeros(dom.N)
+    mask[:, 0] = 1
+    g = s._tr_geometry(bb.Sensor(dom, binary_mask=mask))
+    assert (g.normal_axis, g.normal_value, g.inward) == (1, 0.0, 1.0)

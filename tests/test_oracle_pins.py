@@ -300,3 +300,229 @@ def test_oracle_dopri5_converges_to_dop853_and_honours_max_steps():
     # ending steps on the save times adds nt - 1 to the budget
     *_, status, steps = oo.dopri5(x0, p0, M0, 1.0, 1.0, ts, speed, max_steps=2)
     assert status == 2 and steps == 2 + ts.size - 1
+
+
+# ---- time reversal (tests/solvers/test_tr_solver.py:88-260) ----------------
+
+
+def _tr_1d(mask_idx):
+    from oracle import ode as oo
+    from oracle import tr as otr
+
+    dom = om.Dom(N=(16,), dx=(0.1,), periodic=(False,), c=1.0)
+    wpt = om.Wpt(om.Decomp(1, (16,), (2,), (1,)), 2, "rectangular")
+    pos = np.zeros((1, 1))
+    pos[0, 0] = (np.arange(16) * 0.1)[mask_idx]
+    src = otr.Sources(pos, dom.dx, dom.grid_size)
+    idx = np.arange(min(8, wpt.total_coeffs))
+    return otr.tr_parameters(idx, dom, wpt, src, oo.LinearSpeed(1.0, np.zeros(1)))
+
+
+@pytest.mark.parametrize("mask_idx,sign", [(0, 1.0), (-1, -1.0)])
+def test_tr_beams_point_inward(mask_idx, sign):
+    pts = _tr_1d(mask_idx)[0]
+    n = pts[:, 0]
+    finite = np.abs(n) > 1e-8
+    assert finite.any()
+    assert np.all(sign * n[finite] >= 0)
+
+
+def _tr_2d_data(c, data_dx=(1.0, 1.0)):
+    dom = om.Dom(N=(16, 16), dx=data_dx, periodic=(False, False), c=c)
+    return dom, om.Wpt(om.Decomp(1, (16, 16), (2,), (1, 1)), 2, "rectangular")
+
+
+def test_tr_detector_side_from_spatial_domain():
+    from oracle import ode as oo
+    from oracle import tr as otr
+
+    data_dom, wpt = _tr_2d_data(0.01, (1.0, 0.1))
+    pos = np.stack([np.full(16, 15 * 0.1), np.arange(16) * 0.1], 1)
+    src = otr.Sources(pos, (0.1, 0.1), (1.6, 1.6))
+    idx = np.arange(min(64, wpt.total_coeffs))
+    pts = otr.tr_parameters(idx, data_dom, wpt, src, oo.LinearSpeed(0.01, np.zeros(2)))[0]
+    lvl, mi = om.find_tensor_and_multiindex(idx, om.coeff_shapes(wpt))
+    ch = wpt.dyadic_decomp.centres_ndim[mi[0]] / data_dom.grid_size
+    hyper = ch[:, 0] ** 2 - 0.01 ** 2 * np.sum(ch[:, 1:] ** 2, 1) > 1e-10
+    assert hyper.any()
+    assert np.all(pts[hyper, 0] <= 0)
+
+
+def test_tr_temporal_carrier_sets_tangential_phase():
+    from oracle import ode as oo
+    from oracle import tr as otr
+
+    data_dom, wpt = _tr_2d_data(0.3)
+    pos = np.stack([np.zeros(16), np.arange(16) * 1.0], 1)
+    src = otr.Sources(pos, (1.0, 1.0), (16.0, 16.0))
+    idx = np.arange(min(64, wpt.total_coeffs))
+    pts, _, _, omega, *_ = otr.tr_parameters(idx, data_dom, wpt, src, oo.LinearSpeed(0.3, np.zeros(2)))
+    lvl, mi = om.find_tensor_and_multiindex(idx, om.coeff_shapes(wpt))
+    ch = wpt.dyadic_decomp.centres_ndim[mi[0]] / data_dom.grid_size
+    tau, k_tan = ch[:, 0], ch[:, 1:]
+    ok = (np.abs(tau) > 1e-8) & (np.linalg.norm(k_tan, axis=1) > 1e-8)
+    assert ok.any()
+    np.testing.assert_allclose(omega[ok], np.abs(tau[ok]))
+    np.testing.assert_allclose(omega[ok, None] * pts[ok, 1:], 2 * np.pi * k_tan[ok])
+
+
+@pytest.mark.parametrize("redundancy", [1, 2])
+def test_tr_packet_positions_follow_redundant_anisotropic_support(redundancy):
+    from oracle import ode as oo
+    from oracle import tr as otr
+
+    data_dom = om.Dom(N=(32, 16), dx=(0.1, 0.3), periodic=(False, False), c=0.01)
+    dec = om.Decomp(1, (32, 16), (4,), (2, 1))
+    wpt = om.Wpt(dec, redundancy, "rectangular")
+    pos = np.stack([np.zeros(16), np.arange(16) * 0.3], 1)
+    src = otr.Sources(pos, (0.2, 0.3), (3.2, 4.8))
+    shape = tuple(int(v) for v in wpt.coeff_shapes[0])
+    k = np.array([shape[1] - 1, shape[2] - 1])
+    flat = np.ravel_multi_index((0, k[0], k[1]), shape)
+    _, _, x, _, a, _, t0 = otr.tr_parameters(np.array([flat]), data_dom, wpt, src,
+                                             oo.LinearSpeed(0.01, np.zeros(2)))
+    support = redundancy * dec.box_lengths[0] * np.array([2, 1])
+    expect = k * data_dom.grid_size / support
+    assert t0[0] == pytest.approx(expect[0])
+    assert x[0, 0] == pytest.approx(0.0)
+    assert x[0, 1] == pytest.approx(expect[1])
+    assert t0[0] < data_dom.grid_size[0] and x[0, 1] < data_dom.grid_size[1]
+    ph = om.compute_frame_phase(dec, 0, k, redundancy)
+    assert a[0] / abs(a[0]) == pytest.approx(ph)
+
+
+def test_tr_spatial_hessian_inverts_spacetime_hessian():
+    """mT_inverse (tr_solver_utils.py:116-170) is the inverse of mT_forward
+    (:64-113) for a spatial Hessian whose lower-right block is the
+    spacetime one's."""
+    from oracle import ode as oo
+    from oracle import tr as otr
+
+    rng = np.random.default_rng(0)
+    speed = oo.LinearSpeed(1500.0, np.array([30.0, -20.0]))
+    x = np.array([0.0, 1e-3])
+    p = np.array([3.0, 1.0])
+    S = rng.standard_normal((2, 2)) + 1j * rng.standard_normal((2, 2))
+    S = S + S.T
+    M = otr.mT_inverse(x, p, S, -1.0, speed)
+    gp, gx = otr.gp_gx(x, p, -1.0, speed)
+    xd, pd = gp, -gx
+    # mT_forward of the spatial result gives S back
+    up_left = xd @ M @ xd - pd @ xd
+    up_right = (pd - M @ xd)[1:]
+    # |x_dot|^2 ~ c^2 = 2.25e6 against O(1) entries: cancellation to ~1e-10
+    np.testing.assert_allclose(up_left, S[0, 0], rtol=1e-8)
+    np.testing.assert_allclose(up_right, S[0, 1:], rtol=1e-8)
+    np.testing.assert_allclose(M[1:, 1:], S[1:, 1:])
+
+
+# ---- principal-symbol adjoint (tests/solvers/test_adj_solver_utils.py,
+# ---- tests/solvers/test_msgb_solver_misc.py:452-578) -----------------------
+
+
+def test_b_inverse_normal_incidence_sign_and_conjugacy():
+    from oracle import tr as otr
+
+    b = otr.principal_b_inverse(np.array([3.0, -3.0]), np.zeros((2, 1)), np.array([2.0, 2.0]))
+    assert b[0] == pytest.approx(-1j / (4.0 * np.pi * 2.0 * 3.0))
+    assert b[1] == pytest.approx(np.conj(b[0]))
+
+
+def test_b_inverse_removes_evanescent_and_grazing_modes():
+    from oracle import tr as otr
+
+    r = 5e-7
+    b = otr.principal_b_inverse(np.array([1.0, 2.0, 1.0, 0.0]),
+                                np.array([[1.0], [1.0], [np.sqrt(1.0 - r * r)], [0.0]]),
+                                np.array([2.0, 2.0, 1.0, 1.0]))
+    assert np.all(b == 0.0)
+
+
+def test_b_inverse_relative_guard_is_frequency_local():
+    from oracle import tr as otr
+
+    tau = np.array([1.0, 1e6])
+    b = otr.principal_b_inverse(tau, (tau * np.sqrt(1.0 - 1e-6))[:, None], np.ones(2))
+    assert np.all(np.abs(b) > 0)
+    assert b[0] / b[1] == pytest.approx(tau[1] / tau[0], rel=1e-6)
+
+
+def _adj_2d(c0, grad=0.0):
+    from oracle import ode as oo
+    from oracle import tr as otr
+
+    dom = om.Dom(N=(16, 16), dx=(1.0, 1.0), periodic=(False, False), c=c0)
+    wpt = om.Wpt(om.Decomp(1, (16, 16), (2,), (1, 1)), 2, "rectangular")
+    pos = np.stack([np.zeros(16), np.arange(16.0)], 1)
+    src = otr.Sources(pos, (1.0, 1.0), (16.0, 16.0))
+    return dom, wpt, src, oo.LinearSpeed(c0, np.array([0.0, grad]))
+
+
+def test_adj_parameters_are_tr_geometry_times_b_inverse():
+    from oracle import tr as otr
+
+    dom, wpt, src, speed = _adj_2d(0.3, 0.01)
+    idx = np.array([0, 5, 256, 261])
+    tr = otr.tr_parameters(idx, dom, wpt, src, speed)
+    adj = otr.adj_parameters(idx, dom, wpt, src, speed)
+    lvl, mi = om.find_tensor_and_multiindex(idx, om.coeff_shapes(wpt))
+    ch = wpt.dyadic_decomp.centres_ndim[mi[0]] / dom.grid_size
+    c = np.array([speed.eval(x)[0] for x in adj[2]])
+    binv = -otr.principal_b_inverse(ch[:, 0], ch[:, 1:], c, 5e-2)
+    keep = binv != 0
+    for k in (0, 1, 2, 3, 5, 6):
+        a, b = np.asarray(tr[k]), np.asarray(adj[k])
+        np.testing.assert_allclose(b[keep], a[keep])
+    np.testing.assert_allclose(adj[4], tr[4] * binv)
+
+
+def test_adj_parameters_zero_for_evanescent_packets():
+    from oracle import tr as otr
+
+    dom, wpt, src, speed = _adj_2d(10.0)
+    idx = np.array([0, 256, 512, 768])
+    adj = otr.adj_parameters(idx, dom, wpt, src, speed)
+    assert np.all(adj[4] == 0)
+    assert np.all(adj[0] == 1.0)
+    np.testing.assert_array_equal(adj[1], np.broadcast_to(1j * np.eye(2), adj[1].shape))
+
+
+def test_adj_parameters_1d():
+    from oracle import ode as oo
+    from oracle import tr as otr
+
+    dom = om.Dom(N=(16,), dx=(1.0,), periodic=(False,), c=0.5)
+    wpt = om.Wpt(om.Decomp(1, (16,), (2,), (1,)), 2, "rectangular")
+    src = otr.Sources(np.zeros((1, 1)), (1.0,), (16.0,))
+    speed = oo.LinearSpeed(0.5, np.zeros(1))
+    idx = np.array([0, 16])
+    tr = otr.tr_parameters(idx, dom, wpt, src, speed)
+    adj = otr.adj_parameters(idx, dom, wpt, src, speed)
+    lvl, mi = om.find_tensor_and_multiindex(idx, om.coeff_shapes(wpt))
+    tau = (wpt.dyadic_decomp.centres_ndim[mi[0]] / dom.grid_size)[:, 0]
+    binv = -otr.principal_b_inverse(tau, np.zeros((2, 0)), np.full(2, 0.5), 5e-2)
+    np.testing.assert_allclose(adj[4], tr[4] * binv)
+
+
+def test_adjoint_source_spectral_derivative_sign_and_c_squared():
+    from oracle import tr as otr
+
+    n, dt, mode = 64, 0.25 / 64, 5
+    t = np.arange(n) * dt
+    w = 2 * np.pi * mode / (n * dt)
+    c = np.array([2.0, 3.0])
+    s = otr.form_adjoint_source(np.ones((n, 2)), dt, c, np.sin(w * t))
+    np.testing.assert_allclose(s, -(c ** 2) * w * np.cos(w * t)[:, None], rtol=1e-12, atol=1e-10)
+
+
+def test_adjoint_source_folds_flat_speeds_onto_detector_grid():
+    from oracle import tr as otr
+
+    rng = np.random.default_rng(0)
+    data = rng.standard_normal((8, 3, 2))
+    c = rng.uniform(1.0, 2.0, 6)
+    g = otr.form_adjoint_source(data, 0.1, c)
+    f = otr.form_adjoint_source(data.reshape(8, 6), 0.1, c)
+    np.testing.assert_allclose(g.reshape(8, 6), f, atol=1e-12)
+    with pytest.raises(ValueError, match="does not match the data detector grid"):
+        otr.form_adjoint_source(np.ones((4, 3, 2)), 0.1, np.ones(5))
