@@ -67,6 +67,30 @@ __device__ __forceinline__ cf csqrtf_(cf z) {
     if (z.re >= 0.0f) return cf{r, z.im / (2.0f * r)};
     return cf{fabsf(z.im) / (2.0f * r), copysignf(r, z.im)};
 }
+#ifndef MSGB_F32X2
+#define MSGB_F32X2 1
+#endif
+#if MSGB_F32X2
+// Two complex numbers, component-packed, for the paired FP32 instructions of
+// sm_100 (FFMA2 / FMUL2 / FADD2).  Each lane of a paired operation rounds
+// exactly as the scalar instruction, so these produce the same bits as cmul
+// and kahan_add applied to each half.
+struct cf2 {
+    float2 re, im;
+};
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ cf2 cmul2(cf2 a, cf2 b) {
+    return cf2{__ffma2_rn(a.re, b.re, neg2(__fmul2_rn(a.im, b.im))), __ffma2_rn(a.re, b.im, __fmul2_rn(a.im, b.re))};
+}
+__device__ __forceinline__ void kahan_add2(float2 &acc, float2 &cmp, float2 v) {
+    const float2 y = __fadd2_rn(v, neg2(cmp));
+    const float2 t = __fadd2_rn(acc, y);
+    cmp = __fadd2_rn(__fadd2_rn(t, neg2(acc)), neg2(y));
+    acc = t;
+}
+__device__ __forceinline__ cf2 pack2(cf a, cf b) { return cf2{make_float2(a.re, b.re), make_float2(a.im, b.im)}; }
+#endif
+
 // exp(x + i y) with y range-reduced first.
 __device__ __forceinline__ cf cexpf_(float x, float y) {
     float s, c;
@@ -580,17 +604,22 @@ fwd32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
         const bool fast = gfast_g[st * NW + warp] != 0;
         const int gbase = warp * GS;
         const bool active = gbase < s_cnt;
-        float acc[GS], cmp[GS];
+        // Kahan sums of sensors 2h and 2h + 1 in .x and .y
+        float2 acc2[GS / 2], cmp2[GS / 2];
 #pragma unroll
-        for (int k = 0; k < GS; ++k) acc[k] = 0.0f, cmp[k] = 0.0f;
+        for (int h = 0; h < GS / 2; ++h) acc2[h] = make_float2(0.0f, 0.0f), cmp2[h] = make_float2(0.0f, 0.0f);
         if (TRAJ && !T.first && lane < t_cnt && active) {
             const int64_t t = t_first + lane;
 #pragma unroll
             for (int k = 0; k < GS; ++k) {
                 const int s = gbase + k;
                 if (s < s_cnt) {
-                    acc[k] = T.state[t * P.ns + s_first + s];
-                    cmp[k] = T.state[(P.nt + t) * P.ns + s_first + s];
+                    const float a = T.state[t * P.ns + s_first + s];
+                    const float c = T.state[(P.nt + t) * P.ns + s_first + s];
+                    if (k & 1)
+                        acc2[k / 2].y = a, cmp2[k / 2].y = c;
+                    else
+                        acc2[k / 2].x = a, cmp2[k / 2].x = c;
                 }
             }
         }
@@ -664,23 +693,58 @@ fwd32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
                             if (kb == kRunNegligible) zb = fb = qb = cf{0.0f, 0.0f};
                         }
                         if (fast && ka != kRunDirect && kb != kRunDirect) {
-                            kahan_add(acc[0], cmp[0], za.re + zb.re);
+#if MSGB_F32X2
+                            // z_{k+1} = z_k f_k, f_{k+1} = f_k q for both beams in one
+                            // paired instruction stream; sensors 2h, 2h + 1 share a
+                            // paired Kahan update.
+                            cf2 z = pack2(za, zb), f = pack2(fa, fb);
+                            const cf2 q = pack2(qa, qb);
+#pragma unroll
+                            for (int h = 0; h < GS / 2; ++h) {
+                                if (h > 0) {
+                                    z = cmul2(z, f);
+                                    f = cmul2(f, q);
+                                }
+                                const float v0 = z.re.x + z.re.y;
+                                z = cmul2(z, f);
+                                f = cmul2(f, q);
+                                kahan_add2(acc2[h], cmp2[h], make_float2(v0, z.re.x + z.re.y));
+                            }
+#else
+                            float v[GS];
+                            v[0] = za.re + zb.re;
 #pragma unroll
                             for (int k = 1; k < GS; ++k) {
                                 za = cmul(za, fa);
                                 fa = cmul(fa, qa);
                                 zb = cmul(zb, fb);
                                 fb = cmul(fb, qb);
-                                kahan_add(acc[k], cmp[k], za.re + zb.re);
+                                v[k] = za.re + zb.re;
                             }
-                        } else {
-                            cf dummy_r, dummy_q;
 #pragma unroll
+                            for (int h = 0; h < GS / 2; ++h) {
+                                kahan_add(acc2[h].x, cmp2[h].x, v[2 * h]);
+                                kahan_add(acc2[h].y, cmp2[h].y, v[2 * h + 1]);
+                            }
+#endif
+                        } else {
+                            // Rare (broken runs, out-of-range recurrences): one copy of
+                            // the direct evaluation in a loop, values staged in a small
+                            // array, instead of GS inlined copies (keeps the hot loop
+                            // inside the instruction cache).
+                            cf dummy_r, dummy_q;
+                            float v[GS];
+#pragma unroll 1
                             for (int k = 0; k < GS; ++k) {
                                 const int s = gbase + k;
                                 const cf za = seed_eval<D, PERIODIC>(ra, sds[s], shn[s], false, P, dummy_r, dummy_q);
                                 const cf zb = seed_eval<D, PERIODIC>(rb, sds[s], shn[s], false, P, dummy_r, dummy_q);
-                                kahan_add(acc[k], cmp[k], za.re + zb.re);
+                                v[k] = za.re + zb.re;
+                            }
+#pragma unroll
+                            for (int h = 0; h < GS / 2; ++h) {
+                                kahan_add(acc2[h].x, cmp2[h].x, v[2 * h]);
+                                kahan_add(acc2[h].y, cmp2[h].y, v[2 * h + 1]);
                             }
                         }
                     }
@@ -694,11 +758,13 @@ fwd32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
             for (int k = 0; k < GS; ++k) {
                 const int s = gbase + k;
                 if (s < s_cnt) {
+                    const float a = (k & 1) ? acc2[k / 2].y : acc2[k / 2].x;
+                    const float c = (k & 1) ? cmp2[k / 2].y : cmp2[k / 2].x;
                     if (TRAJ && !T.last) {
-                        T.state[t * P.ns + s_first + s] = acc[k];
-                        T.state[(P.nt + t) * P.ns + s_first + s] = cmp[k];
+                        T.state[t * P.ns + s_first + s] = a;
+                        T.state[(P.nt + t) * P.ns + s_first + s] = c;
                     } else {
-                        out[t * P.ns + perm[s_first + s]] = acc[k] - cmp[k];
+                        out[t * P.ns + perm[s_first + s]] = a - c;
                     }
                 }
             }
@@ -709,175 +775,204 @@ fwd32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
 }
 
 // ------------------------------------------------------------------ adjoint
-// One warp per selected coefficient (both modes), lanes = the 32 times of a
-// time tile.  Lanes test 32 sensor tiles at a time; for each surviving tile
-// every lane accumulates d(t, s) conj(z) over the tile's sensors: groups that
-// are single runs are walked four at a time with interleaved recurrence
-// chains (data for the next sensor is loaded one step ahead), the others by
-// direct evaluation.  Data is in sorted-sensor-major layout (lanes read
-// consecutive times).  Per-tile FP32 partials go into FP64; the warp result is
-// reduced in a fixed order, so the output is deterministic.
+// Tile-parallel transpose.  Persistent CTAs take (time tile, sensor tile)
+// items as the forward does; warp w owns sensor group w and lane l time l,
+// and holds d(t, s) for its GS sensors in registers for the whole item.  Each
+// pair of surviving beams runs the forward's recurrence while the lane
+// accumulates sum_s d(t, s) conj(z(t, s)); the pair's partials are reduced
+// over the 32 times (FP64 shuffles, fixed order), over the warps (FP64, fixed
+// order) and added to the beam's FP64 slot with one atomic per (beam, item).
+// g must be zeroed first; the order of those atomic additions varies between
+// runs (last-bit differences of the FP64 result).
 template <int D, bool PERIODIC, bool TRAJ>
-__global__ void __launch_bounds__(THREADS)
+__global__ void __launch_bounds__(THREADS, 2)
 adj32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *tiles, const int32_t *offs,
-             int64_t n_st, const float *ds_g, const float *hn_g, const uint8_t *gfast_g, const float *dataT,
-             float cutoff, double *g, unsigned long long *eval_count, unsigned long long *work, TrajSrc<D> T) {
-    constexpr int CH = 4;
-    const int lane = threadIdx.x & 31;
-    const int64_t n_owned = TRAJ ? T.nb : B.n;
+             const float *ds_g, const float *hn_g, const uint8_t *gfast_g, const float *dataT, float cutoff,
+             double *g, unsigned long long *eval_count, int *work, int n_st, int n_tiles, TrajSrc<D> T) {
+    constexpr int NF = Rec<D>::NF;
+    __shared__ float rec[NF][G][TT];
+    __shared__ float sds[TS][D], shn[TS][D];
+    __shared__ int64_t surv[2 * THREADS];
+    __shared__ int warp_cnt[NW];
+    __shared__ double part[NW][G][2];
+    __shared__ int tile_s, nsurv_s;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     unsigned long long evals = 0;
-    // Persistent warps: each takes the next beam from a global counter, so
-    // the uneven per-beam work (coarse beams cross many more tiles) does not
-    // leave warps idle at the end of a statically assigned block.
-    for (;;) {
-    unsigned long long jj = 0;
-    if (lane == 0) jj = atomicAdd(work, 1ull);
-    const int64_t j = (int64_t)__shfl_sync(0xffffffffu, jj, 0);
-    if (j >= n_owned) break;
-    const Cull<D> cb = TRAJ ? Cull<D>{} : cull[j];
-    const int64_t n_tt = (P.nt + TT - 1) / TT;
-    double gre = 0.0, gim = 0.0;
-    for (int m = 0; m < (TRAJ ? 1 : 2); ++m) {
-        if (!TRAJ && !mode_on(B.modes, m)) continue;
-        const float c0 = m == 0 ? (float)P.c : -(float)P.c;
-        const int64_t b = m == 0 ? j : j + B.n;
-        for (int64_t tt = 0; tt < n_tt; ++tt) {
-            const int64_t t_first = tt * TT;
-            const int t_cnt = (int)min((int64_t)TT, P.nt - t_first);
-            const float ta = (float)P.ts[t_first], tb = (float)P.ts[t_first + t_cnt - 1];
-            const bool tv = lane < t_cnt;
-            const int64_t t = t_first + (tv ? lane : 0);
-            bool have_bt = false;
-            BeamTime<D> bt;
-            for (int64_t st0 = 0; st0 < n_st; st0 += 32) {
-                const int64_t st_l = st0 + lane;
-                bool keep = false;
-                if (st_l < n_st)
-                    keep = TRAJ ? traj_survives<D>(T, j, tt, tiles[st_l], cutoff)
-                                : survives<D>(cb, c0, ta, tb, tiles[st_l], P, cutoff);
-                unsigned mask = __ballot_sync(0xffffffffu, keep);
-                if (mask && !have_bt) {
-                    if (TRAJ)
-                        traj_beam_time<D>(B, T, j, t, bt);
-                    else
-                        beam_time<D>(P, B, b, P.ts[t], bt);
-                    have_bt = true;
+    while (true) {
+        if (tid == 0) tile_s = atomicAdd(work, 1);
+        __syncthreads();
+        const int tile = tile_s;
+        if (tile >= n_tiles) break;
+        const int64_t st = tile % n_st, tt = tile / n_st;
+        const int64_t s_first = offs[st], t_first = tt * TT;
+        const int s_cnt = offs[st + 1] - offs[st];
+        const int t_cnt = (int)min((int64_t)TT, P.nt - t_first);
+        const TileInfo<D> ti = tiles[st];
+        const float ta = (float)P.ts[t_first], tb = (float)P.ts[t_first + t_cnt - 1];
+        for (int k = tid; k < TS; k += THREADS) {
+#pragma unroll
+            for (int i = 0; i < D; ++i) {
+                sds[k][i] = k < s_cnt ? ds_g[(s_first + k) * D + i] : 0.0f;
+                shn[k][i] = k < s_cnt ? hn_g[(s_first + k) * D + i] : 0.0f;
+            }
+        }
+        const bool fast = gfast_g[st * NW + warp] != 0;
+        const int gbase = warp * GS;
+        const bool active = gbase < s_cnt;
+        const bool tv = lane < t_cnt;
+        const float *dcol = dataT + (int64_t)s_first * P.nt + t_first + lane;
+        float dv[GS];
+#pragma unroll
+        for (int k = 0; k < GS; ++k)
+            dv[k] = (tv && gbase + k < s_cnt) ? __ldg(dcol + (int64_t)(gbase + k) * P.nt) : 0.0f;
+        const int64_t nbeam = TRAJ ? T.nb : B.n;
+
+        for (int64_t j0 = 0; j0 < nbeam; j0 += THREADS) {
+            const int64_t j = j0 + tid;
+            bool keep_p = false, keep_m = false;
+            if (j < nbeam) {
+                if (TRAJ) {
+                    keep_p = traj_survives<D>(T, j, tt, ti, cutoff);
+                } else {
+                    const Cull<D> cb = cull[j];
+                    keep_p = mode_on(B.modes, 0) && survives<D>(cb, (float)P.c, ta, tb, ti, P, cutoff);
+                    keep_m = mode_on(B.modes, 1) && survives<D>(cb, -(float)P.c, ta, tb, ti, P, cutoff);
                 }
-                while (mask) {
-                    const int k = __ffs(mask) - 1;
-                    mask &= mask - 1;
-                    const int64_t st = st0 + k;
-                    const int64_t s_first = offs[st];
-                    const int s_cnt = offs[st + 1] - offs[st];
-                    const TileInfo<D> ti = tiles[st];
+            }
+            const unsigned bp = __ballot_sync(0xffffffffu, keep_p);
+            const unsigned bm = __ballot_sync(0xffffffffu, keep_m);
+            if (lane == 0) warp_cnt[warp] = __popc(bp) + __popc(bm);
+            __syncthreads();
+            int off = 0, tot = 0;
+#pragma unroll
+            for (int w = 0; w < NW; ++w) {
+                if (w < warp) off += warp_cnt[w];
+                tot += warp_cnt[w];
+            }
+            const unsigned lt = (1u << lane) - 1u;
+            if (keep_p) surv[off + __popc(bp & lt)] = j;
+            if (keep_m) surv[off + __popc(bp) + __popc(bm & lt)] = j + B.n;
+            if (tid == 0) nsurv_s = tot;
+            __syncthreads();
+            const int nsurv = nsurv_s;
+            evals += (unsigned long long)nsurv * (unsigned long long)t_cnt * (unsigned long long)s_cnt;
+            for (int g0 = 0; g0 < nsurv; g0 += G) {
+                {
+                    const int gl = tid / TT, tloc = tid % TT;
                     Rec<D> r;
-                    anchor<D>(P, bt, ti.s0, r);
-                    if (!tv) r.amp = 0.0f;
-                    float pr = 0.0f, pi = 0.0f;
-                    const float *dcol = dataT + s_first * P.nt + t;
-                    const int ngroups = (s_cnt + GS - 1) / GS;
-                    unsigned fastbits = 0;
-                    for (int gq = 0; gq < ngroups; ++gq) fastbits |= (unsigned)(__ldg(gfast_g + st * NW + gq) != 0) << gq;
-                    int gq = 0;
-                    while (gq < ngroups) {
-                        if (gq + CH <= ngroups && ((fastbits >> gq) & ((1u << CH) - 1u)) == ((1u << CH) - 1u)) {
-                            cf z[CH], rr[CH], qq[CH];
-                            float d[CH];
-                            bool ok = true;
+                    if (g0 + gl < nsurv && tloc < t_cnt) {
+                        BeamTime<D> bt;
+                        if (TRAJ)
+                            traj_beam_time<D>(B, T, surv[g0 + gl], t_first + tloc, bt);
+                        else
+                            beam_time<D>(P, B, surv[g0 + gl], P.ts[t_first + tloc], bt);
+                        anchor<D>(P, bt, ti.s0, r);
+                    } else {
 #pragma unroll
-                            for (int c = 0; c < CH; ++c) {
-                                const int s = (gq + c) * GS;
-                                float dsl[D], hl[D];
+                        for (int i = 0; i < D; ++i) r.d0[i] = 0.0f, r.wp[i] = 0.0f;
 #pragma unroll
-                                for (int i = 0; i < D; ++i)
-                                    dsl[i] = __ldg(ds_g + (s_first + s) * D + i), hl[i] = __ldg(hn_g + (s_first + s) * D + i);
-                                int kc = kRunRecurrence;
-                                z[c] = seed_eval<D, false>(r, dsl, hl, true, P, rr[c], qq[c], &kc, cutoff > 0.0f);
-                                if (kc == kRunNegligible) z[c] = rr[c] = qq[c] = cf{0.0f, 0.0f};
-                                ok = ok && kc != kRunDirect;
-                                d[c] = tv ? __ldg(dcol + (int64_t)s * P.nt) : 0.0f;
-                            }
-                            if (!ok) {
-                                // out-of-range recurrence: these CH groups sensor by sensor
-                                for (int s = gq * GS; s < (gq + CH) * GS; ++s) {
-                                    float dsl[D], hl[D];
+                        for (int q = 0; q < Sym<D>::S; ++q) r.q[q] = 0.0f, r.p[q] = 0.0f;
+                        r.th0 = 0.0f;
+                        r.amp = 0.0f;
+                    }
+                    const float *rf = reinterpret_cast<const float *>(&r);
 #pragma unroll
-                                    for (int i = 0; i < D; ++i)
-                                        dsl[i] = __ldg(ds_g + (s_first + s) * D + i), hl[i] = 0.0f;
-                                    cf dr, dq;
-                                    const cf zd = seed_eval<D, false>(r, dsl, hl, false, P, dr, dq);
-                                    const float dd = tv ? __ldg(dcol + (int64_t)s * P.nt) : 0.0f;
-                                    pr = fmaf(dd, zd.re, pr);
-                                    pi = fmaf(-dd, zd.im, pi);
+                    for (int f = 0; f < NF; ++f) rec[f][gl][tloc] = rf[f];
+                }
+                __syncthreads();
+                const int ng = min(G, nsurv - g0);
+                for (int gl = 0; gl < ng; gl += 2) {
+                    float2 ar = make_float2(0.0f, 0.0f), ai = make_float2(0.0f, 0.0f);
+                    if (active) {
+                        Rec<D> ra, rb;
+                        load_rec<D>(rec, gl, lane, ra);
+                        load_rec<D>(rec, gl + 1, lane, rb);  // zero-amplitude record when gl + 1 == ng
+                        cf za, fa, qa, zb, fb, qb;
+                        int ka = kRunRecurrence, kb = kRunRecurrence;
+                        if (fast) {
+                            za = seed_eval<D, false>(ra, sds[gbase], shn[gbase], true, P, fa, qa, &ka, cutoff > 0.0f);
+                            zb = seed_eval<D, false>(rb, sds[gbase], shn[gbase], true, P, fb, qb, &kb, cutoff > 0.0f);
+                            if (ka == kRunNegligible) za = fa = qa = cf{0.0f, 0.0f};
+                            if (kb == kRunNegligible) zb = fb = qb = cf{0.0f, 0.0f};
+                        }
+                        if (fast && ka != kRunDirect && kb != kRunDirect) {
+#if MSGB_F32X2
+                            cf2 z = pack2(za, zb), f = pack2(fa, fb);
+                            const cf2 q = pack2(qa, qb);
+#pragma unroll
+                            for (int k = 0; k < GS; ++k) {
+                                if (k > 0) {
+                                    z = cmul2(z, f);
+                                    f = cmul2(f, q);
                                 }
-                                gq += CH;
-                                continue;
+                                const float2 dk = make_float2(dv[k], dv[k]);
+                                ar = __ffma2_rn(dk, z.re, ar);
+                                ai = __ffma2_rn(neg2(dk), z.im, ai);
                             }
-                            float d1[CH], ar[CH], ai[CH];
+#else
 #pragma unroll
-                            for (int c = 0; c < CH; ++c) {
-                                d1[c] = tv ? __ldg(dcol + (int64_t)((gq + c) * GS + 1) * P.nt) : 0.0f;
-                                ar[c] = 0.0f;
-                                ai[c] = 0.0f;
-                            }
-#pragma unroll 4
-                            for (int kk = 0; kk < GS; ++kk) {
-                                float dn[CH];
-#pragma unroll
-                                for (int c = 0; c < CH; ++c)
-                                    dn[c] = (tv && kk + 2 < GS) ? __ldg(dcol + (int64_t)((gq + c) * GS + kk + 2) * P.nt) : 0.0f;
-#pragma unroll
-                                for (int c = 0; c < CH; ++c) {
-                                    ar[c] = fmaf(d[c], z[c].re, ar[c]);
-                                    ai[c] = fmaf(-d[c], z[c].im, ai[c]);
-                                    z[c] = cmul(z[c], rr[c]);
-                                    rr[c] = cmul(rr[c], qq[c]);
-                                    d[c] = d1[c];
-                                    d1[c] = dn[c];
+                            for (int k = 0; k < GS; ++k) {
+                                if (k > 0) {
+                                    za = cmul(za, fa);
+                                    fa = cmul(fa, qa);
+                                    zb = cmul(zb, fb);
+                                    fb = cmul(fb, qb);
                                 }
+                                ar.x = fmaf(dv[k], za.re, ar.x);
+                                ai.x = fmaf(-dv[k], za.im, ai.x);
+                                ar.y = fmaf(dv[k], zb.re, ar.y);
+                                ai.y = fmaf(-dv[k], zb.im, ai.y);
                             }
-#pragma unroll
-                            for (int c = 0; c < CH; ++c) {
-                                pr += ar[c];
-                                pi += ai[c];
-                            }
-                            gq += CH;
+#endif
                         } else {
-                            const int s_end = min(s_cnt, (gq + 1) * GS);
-                            for (int s = gq * GS; s < s_end; ++s) {
-                                float dsl[D], hl[D];
-#pragma unroll
-                                for (int i = 0; i < D; ++i)
-                                    dsl[i] = __ldg(ds_g + (s_first + s) * D + i), hl[i] = 0.0f;
-                                cf dr, dq;
-                                const cf z = seed_eval<D, PERIODIC>(r, dsl, hl, false, P, dr, dq);
-                                const float d = tv ? __ldg(dcol + (int64_t)s * P.nt) : 0.0f;
-                                pr = fmaf(d, z.re, pr);
-                                pi = fmaf(-d, z.im, pi);
+                            // rare: broken runs, out-of-range recurrences
+                            cf dummy_r, dummy_q;
+#pragma unroll 1
+                            for (int k = 0; k < GS; ++k) {
+                                const int s = gbase + k;
+                                const float d = (tv && s < s_cnt) ? __ldg(dcol + (int64_t)s * P.nt) : 0.0f;
+                                const cf za = seed_eval<D, PERIODIC>(ra, sds[s], shn[s], false, P, dummy_r, dummy_q);
+                                const cf zb = seed_eval<D, PERIODIC>(rb, sds[s], shn[s], false, P, dummy_r, dummy_q);
+                                ar.x = fmaf(d, za.re, ar.x);
+                                ai.x = fmaf(-d, za.im, ai.x);
+                                ar.y = fmaf(d, zb.re, ar.y);
+                                ai.y = fmaf(-d, zb.im, ai.y);
                             }
-                            gq += 1;
                         }
                     }
-                    gre += (double)pr;
-                    gim += (double)pi;
-                    evals += tv ? (unsigned long long)s_cnt : 0ull;
+                    double v[4] = {(double)ar.x, (double)ai.x, (double)ar.y, (double)ai.y};
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
+                    if (lane == 0) {
+                        part[warp][gl][0] = v[0];
+                        part[warp][gl][1] = v[1];
+                        if (gl + 1 < G) {
+                            part[warp][gl + 1][0] = v[2];
+                            part[warp][gl + 1][1] = v[3];
+                        }
+                    }
+                }
+                __syncthreads();
+                if (tid < ng) {
+                    double re = 0.0, im = 0.0;
+#pragma unroll
+                    for (int w = 0; w < NW; ++w) {
+                        re += part[w][tid][0];
+                        im += part[w][tid][1];
+                    }
+                    const int64_t b = surv[g0 + tid];
+                    const int64_t slot = TRAJ ? b : (b < B.n ? b : b - B.n);
+                    if (re != 0.0) atomicAdd(g + 2 * slot, re);
+                    if (im != 0.0) atomicAdd(g + 2 * slot + 1, im);
                 }
             }
         }
+        __syncthreads();
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        gre += __shfl_down_sync(0xffffffffu, gre, o);
-        gim += __shfl_down_sync(0xffffffffu, gim, o);
-    }
-    if (lane == 0) {
-        g[2 * j] = gre;
-        g[2 * j + 1] = gim;
-    }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) evals += __shfl_down_sync(0xffffffffu, evals, o);
-    if (lane == 0 && eval_count && evals) atomicAdd(eval_count, evals);
+    if (eval_count && tid == 0 && evals) atomicAdd(eval_count, evals);
 }
 
 // ------------------------------------------------------------------ workspace
@@ -1035,17 +1130,20 @@ int run_adj(const msgb_problem *p, const msgb_beam_set *b, const msgb_sum_opts *
     bool periodic = false;
     for (int i = 0; i < D; ++i) periodic |= (p->periodic[i] != 0);
     const int64_t nw = TRAJ ? T.nb : b->n;
-    unsigned long long *work = (unsigned long long *)(ws + l.work + 8);
-    cudaMemsetAsync(work, 0, sizeof(unsigned long long), st);
+    const int64_t n_st = l.n_st, n_tt = (p->nt + TT - 1) / TT;
+    if (n_st * n_tt > 0x7fffffffLL) return fail(MSGB_ERR_UNSUPPORTED, "msgb_adj_gather_f32: too many tiles");
+    cudaMemsetAsync(g, 0, sizeof(double) * 2 * nw, st);
+    int *work = (int *)(ws + l.work);
+    cudaMemsetAsync(work, 0, sizeof(int), st);
+    const int n_tiles = (int)(n_st * n_tt);
     const int64_t want = 2LL * sm_count();
-    const int64_t need = (nw + NW - 1) / NW;
-    const unsigned grid = (unsigned)(need < want ? need : want);
+    const unsigned grid = (unsigned)(want < n_tiles ? want : n_tiles);
     auto args = [&](auto kern) {
         kern<<<grid, THREADS, 0, st>>>(P, to_args(b), (const Cull<D> *)(ws + l.cull), (const TileInfo<D> *)(ws + l.tiles),
-                                       (const int32_t *)(ws + l.offs), l.n_st, (const float *)(ws + l.ds),
+                                       (const int32_t *)(ws + l.offs), (const float *)(ws + l.ds),
                                        (const float *)(ws + l.hn), (const uint8_t *)(ws + l.gfast),
                                        (const float *)(ws + l.data), o ? (float)o->cutoff : 0.0f, g,
-                                       o ? o->eval_count : nullptr, work, T);
+                                       o ? o->eval_count : nullptr, work, (int)n_st, n_tiles, T);
     };
     if (periodic)
         args(adj32_kernel<D, true, TRAJ>);
