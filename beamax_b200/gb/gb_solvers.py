@@ -5,7 +5,13 @@ The reference passes Python functions (beamax gb/gb_solvers.py:356-422
 identifiers that select a libmsgb propagation kernel:
 
 * ``solve_hom_diag`` - closed-form homogeneous propagation (Sherman-Morrison
-  Hessian, closed-form amplitude), fused into the summation kernels.
+  Hessian, closed-form amplitude), fused into the summation kernels.  As in
+  the reference, the speed is c at the origin (``c(zeros(d))``, :356-422) and
+  the absorption ``lam`` is ignored, whatever the medium.
+* ``solve_hom_general`` - the closed form for a general initial Hessian
+  (:425-481: M0 (I + c t P_perp M0 / |p|)^-1, a0 / sqrt(det(...))).  The
+  solver's beams start with a diagonal Hessian, for which it equals
+  ``solve_hom_diag``, so it selects the same fused kernels.
 * ``solve_ODE_base`` - the general ray/Riccati/amplitude ODE.  In a
   homogeneous medium its exact solution is the closed form above, so the same
   fused kernels are used; heterogeneous media use ``msgb_ode_trajectories``
@@ -38,8 +44,12 @@ class SolverId:
 solve_hom_diag = SolverId("solve_hom_diag")
 solve_ODE_base = SolverId("solve_ODE_base")
 solve_ODE_batch_t = SolverId("solve_ODE_batch_t")
+solve_hom_general = SolverId("solve_hom_general")
+solve_hom_TR = SolverId("solve_hom_TR")
 
-KNOWN = {"solve_hom_diag", "solve_ODE_base", "solve_ODE_batch_t"}
+KNOWN = {"solve_hom_diag", "solve_hom_general", "solve_ODE_base", "solve_ODE_batch_t", "solve_hom_TR"}
+# propagators that are closed forms at c(0) (no ODE, absorption ignored)
+CLOSED_FORM = {"solve_hom_diag", "solve_hom_general"}
 
 
 def solver_name(fn) -> str:

@@ -37,7 +37,7 @@ import numpy as np
 from .. import _lib
 from .._device import DeviceCache, as_device_f64, default_device, workspace
 from ..geometry import Domain, Sensor
-from ..gb.gb_solvers import SolverConfig, solver_name
+from ..gb.gb_solvers import CLOSED_FORM, SolverConfig, solver_name
 from ..transforms import MSWPT
 
 _cache = DeviceCache()
@@ -175,6 +175,7 @@ class MSGBSolver:
         self.input_type = input_type
         self.ode_solver = ode_solver
         self.ode_solver_name = solver_name(ode_solver)
+        self.closed_form = self.ode_solver_name in CLOSED_FORM
         self.tr_ode_solver = ode_solver if tr_ode_solver is None else tr_ode_solver
         self.sharding = sharding
         if ode_config is None:
@@ -227,9 +228,13 @@ class MSGBSolver:
         import torch
 
         kind, m = domain.medium()
-        c = float(m) if kind == "constant" else float(np.max(m.values))  # unused by the trajectory kernels
-        if kind == "constant" and domain.lam != 0.0:
-            raise NotImplementedError("absorption (lam != 0) needs the ODE path (heterogeneous media)")
+        if kind == "constant":
+            c = float(m)
+        elif self.closed_form:
+            # solve_hom_diag / solve_hom_general propagate at c(0) (gb_solvers.py:356-422)
+            c = float(np.asarray(m(np.zeros((1, domain.ndim)))).ravel()[0])
+        else:
+            c = float(np.max(m.values))  # unused by the trajectory kernels
         pos = np.ascontiguousarray(self._sensor_positions(sensors), np.float64)
         if pos.ndim != 2 or pos.shape[1] != domain.ndim:
             raise ValueError(f"sensor positions must have shape (Ns, {domain.ndim})")
@@ -413,6 +418,12 @@ class MSGBSolver:
     @staticmethod
     def heterogeneous(domain: Domain) -> bool:
         return domain.medium()[0] != "constant" or domain.lam != 0.0
+
+    def _integrates(self, domain: Domain) -> bool:
+        """The beams go through the ODE kernels: a heterogeneous or absorbing
+        medium with an ODE propagator (the closed forms ignore both, as the
+        reference's do)."""
+        return not self.closed_form and self.heterogeneous(domain)
 
     def _chunks(self, domain: Domain, nt: int, nbeam: int, fp64: bool):
         d = domain.ndim
@@ -600,7 +611,7 @@ class MSGBSolver:
         """Beam summation at the sensors: (Nt, Ns) float64 (fp64) or float32 (fp32)."""
         import torch
 
-        if self.heterogeneous(domain):
+        if self._integrates(domain):
             return self._sum_forward_het(bt, domain, sensors, ts)
 
         dev = bt.x0.device
@@ -629,7 +640,7 @@ class MSGBSolver:
         """Per selected coefficient g_j = sum 2 d conj(K_j) over both modes: (n,) complex128."""
         import torch
 
-        if self.heterogeneous(domain):
+        if self._integrates(domain):
             return self._gather_adjoint_het(bt, domain, sensors, ts, data, _cached)
 
         dev = bt.x0.device
@@ -816,7 +827,7 @@ class MSGBSolver:
         # Gather in flat-index order: neighbouring coefficients (same box,
         # adjacent packet positions) have overlapping footprints, so the
         # per-beam warps of a CTA reuse the same data tiles from L1.
-        cached = self._cached_trajectories(selection, domain, ts) if self.heterogeneous(domain) else None
+        cached = self._cached_trajectories(selection, domain, ts) if self._integrates(domain) else None
         if cached is not None:
             sel_sorted = selection  # the order of the kept trajectory records
         else:

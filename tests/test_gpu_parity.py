@@ -348,3 +348,35 @@ def test_autograd_backward_is_adjoint():
     (y * g).sum().backward()
     ref = solver.adjoint(g, d, sens, ts, w, selection=solver.last_selection)
     assert torch.allclose(x.grad, ref, rtol=0, atol=0)
+
+
+def test_closed_form_propagators_use_c_at_origin_and_ignore_absorption():
+    """solve_hom_diag and solve_hom_general (gb/gb_solvers.py:356-481) take
+    c(0) and ignore lam whatever the medium: the forward on a B-spline medium
+    with absorption equals the forward on the constant medium c(0) (same
+    kernels, bit for bit), and solve_hom_general equals solve_hom_diag."""
+    import beamax_b200 as bb
+    from scipy import ndimage
+
+    from beamax_b200.utils.interp import make_c_function_from_grid
+
+    _dev()
+    N, dx = (64, 64), (1e-4, 1e-4)
+    g = ndimage.gaussian_filter(np.random.default_rng(3).standard_normal(N), 6.0, mode="wrap")
+    cgrid = 1500.0 * (1 + 0.05 * g / np.max(np.abs(g)))
+    interp = make_c_function_from_grid(cgrid, dx, method="bspline3", boundary="clamp")
+    c0 = float(np.asarray(interp(np.zeros((1, 2)))).ravel()[0])
+    het = bb.Domain(N=N, dx=dx, periodic=(False, False), cfl=0.3, c=interp, lam=1e3)
+    hom = bb.Domain(N=N, dx=dx, periodic=(False, False), cfl=0.3, c=c0)
+    wpt = bb.MSWPT(bb.DyadicDecomposition(2, N, (4, 8), (1, 1)), 2, "rectangular_mirror")
+    mask = np.zeros(N)
+    mask[0, :] = 1
+    ts = hom.generate_time_domain()
+    p0 = np.random.default_rng(4).standard_normal(N)
+    gs = bb.gb.gb_solvers
+    outs = []
+    for dom, ode in ((het, gs.solve_hom_diag), (hom, gs.solve_hom_diag), (het, gs.solve_hom_general)):
+        s = bb.MSGBSolver(256, "top_n", 64, "spatial", ode, "scan_real")
+        outs.append(np.asarray(s.forward(p0, dom, bb.Sensor(dom, binary_mask=mask), ts, wpt)))
+    assert np.array_equal(outs[0], outs[1])
+    assert np.array_equal(outs[2], outs[0])

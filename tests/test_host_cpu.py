@@ -230,3 +230,13 @@ def test_time_reversal_detector_geometry():
     mask[:, 0] = 1
     g = s._tr_geometry(bb.Sensor(dom, binary_mask=mask))
     assert (g.normal_axis, g.normal_value, g.inward) == (1, 0.0, 1.0)
+
+
+def test_reference_propagator_names_are_accepted():
+    """gb_solvers.solve_hom_general and solve_hom_TR (gb/gb_solvers.py:425-594)
+    are accepted by name or object; the closed forms are marked as such."""
+    gs = bb.gb.gb_solvers
+    for ode, closed in ((gs.solve_hom_general, True), ("solve_hom_general", True), (gs.solve_hom_diag, True),
+                        (gs.solve_ODE_base, False)):
+        s = bb.MSGBSolver(8, "top_n", 8, "spatial", ode, "scan_real", tr_ode_solver=gs.solve_hom_TR)
+        assert s.closed_form is closed
