@@ -99,6 +99,108 @@ __device__ __forceinline__ void axpy(State<D> &o, const State<D> &y, double h, c
     o.A = y.A + h * k.A;
 }
 
+// The adaptive integrator's state: M is complex symmetric, so only its upper
+// triangle (sym_index order) is carried -- D(D+1)/2 entries instead of D^2,
+// fewer registers per stage and fewer terms in the Riccati right-hand side.
+template <int D>
+struct SState {
+    static constexpr int S = D * (D + 1) / 2;
+    double x[D], p[D];
+    cd M[S];
+    cd A;
+};
+
+template <int D>
+__device__ __forceinline__ void to_full(const SState<D> &s, State<D> &f) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+        f.x[i] = s.x[i];
+        f.p[i] = s.p[i];
+#pragma unroll
+        for (int k = 0; k < D; ++k) f.M[i][k] = s.M[sym_index<D>(i, k)];
+    }
+    f.A = s.A;
+}
+
+template <int D>
+__device__ __forceinline__ void from_full(const State<D> &f, SState<D> &s) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+        s.x[i] = f.x[i];
+        s.p[i] = f.p[i];
+#pragma unroll
+        for (int k = i; k < D; ++k) s.M[sym_index<D>(i, k)] = f.M[i][k];
+    }
+    s.A = f.A;
+}
+
+// coupled_rhs_absorption on the symmetric state (the same terms as rhs; dM
+// is formed for i <= k only).
+template <int D>
+__device__ void rhs_sym(const MediumArgs &med, double mode, const SState<D> &y, SState<D> &dy) {
+    double c, gc[D], hc[D * D];
+    speed_eval<D>(med, y.x, c, gc, hc);
+    double n2 = 0.0;
+#pragma unroll
+    for (int i = 0; i < D; ++i) n2 += y.p[i] * y.p[i];
+    const double np = sqrt(n2);
+    const double np3 = np * n2;
+    const double G = mode * c * np;
+    double Gx[D], Gp[D];
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+        Gx[i] = mode * gc[i] * np;
+        Gp[i] = mode * c * y.p[i] / np;
+        dy.x[i] = Gp[i];
+        dy.p[i] = -Gx[i];
+    }
+    double Gpp[D][D], Gxp[D][D];
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            Gpp[i][k] = mode * c * ((i == k ? 1.0 / np : 0.0) - y.p[i] * y.p[k] / np3);
+            Gxp[i][k] = mode * gc[i] * y.p[k] / np;
+        }
+    cd MG[D][D];
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            cd sacc = cd{0.0, 0.0};
+#pragma unroll
+            for (int l = 0; l < D; ++l) sacc = sacc + Gpp[l][k] * y.M[sym_index<D>(i, l)];
+            MG[i][k] = sacc;
+        }
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int k = i; k < D; ++k) {
+            cd sacc = cd{mode * hc[i * D + k] * np, 0.0};
+#pragma unroll
+            for (int l = 0; l < D; ++l) {
+                sacc = sacc + Gxp[i][l] * y.M[sym_index<D>(l, k)];
+                sacc = sacc + Gxp[k][l] * y.M[sym_index<D>(i, l)];
+                sacc = sacc + MG[i][l] * y.M[sym_index<D>(l, k)];
+            }
+            dy.M[sym_index<D>(i, k)] = cd{-sacc.re, -sacc.im};
+        }
+    cd trM = cd{0.0, 0.0};
+    double gxgp = 0.0;
+    cd gpmgp = cd{0.0, 0.0};
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+        trM = trM + y.M[sym_index<D>(i, i)];
+        gxgp += Gx[i] * Gp[i];
+#pragma unroll
+        for (int k = 0; k < D; ++k) gpmgp = gpmgp + (Gp[i] * Gp[k]) * y.M[sym_index<D>(i, k)];
+    }
+    cd num = (c * c) * trM;
+    num = cd{num.re - gxgp - gpmgp.re + med.lam * G, num.im - gpmgp.im};
+    const cd f = (-1.0 / (2.0 * G)) * num;
+    dy.A = y.A * f;
+}
+
 template <int D>
 __device__ void rk4_step(const MediumArgs &med, double mode, State<D> &y, double h) {
     State<D> k1, k2, k3, k4, t;
@@ -154,9 +256,28 @@ struct NV {
 };
 
 template <int D>
+struct NVS {
+    static constexpr int value = 2 * D + 2 * SState<D>::S + 2;  // doubles in SState<D>
+};
+
+template <int D>
 __device__ __forceinline__ double *vals(State<D> &s) { return reinterpret_cast<double *>(&s); }
 template <int D>
 __device__ __forceinline__ const double *vals(const State<D> &s) { return reinterpret_cast<const double *>(&s); }
+template <int D>
+__device__ __forceinline__ double *vals(SState<D> &s) { return reinterpret_cast<double *>(&s); }
+template <int D>
+__device__ __forceinline__ const double *vals(const SState<D> &s) { return reinterpret_cast<const double *>(&s); }
+
+// Weight of entry e of the symmetric state in the error norm: an
+// off-diagonal M entry stands for two entries of the full matrix.
+template <int D>
+__host__ __device__ constexpr double sym_weight(int e) {
+    return (e < 2 * D || e >= 2 * D + SState<D>::S) ? 1.0
+         : (D == 2 ? (e - 2 * D == 1 ? 2.0 : 1.0)
+         : D == 3 ? ((e - 2 * D == 1 || e - 2 * D == 2 || e - 2 * D == 4) ? 2.0 : 1.0)
+         : 1.0);
+}
 
 // Magnitude of complex entry e of the state (x and p entries are real).
 template <int D>
@@ -184,7 +305,7 @@ __constant__ double DP_D[7] = {-12715105075.0 / 11282082432.0, 0.0, 87487479700.
 //      continuous extension, as diffrax's SaveAt(ts) reads its interpolant.
 template <int D>
 struct DopriBeam {
-    State<D> y, f0;
+    SState<D> y, f0;
     double t, h, mode;
     int64_t steps, k;
     bool rejected;
@@ -198,15 +319,16 @@ struct DopriBeam {
         k = 1;
         rejected = false;
         code = 0;
-        rhs<D>(med, mode, y, f0);
+        rhs_sym<D>(med, mode, y, f0);
     }
 
     // One attempt; returns true when the beam is finished (all save times
     // written or the step budget exhausted).
     __device__ bool attempt(const MediumArgs &med, const ProbArgs &P, const OdeArgs &o, RecordWriter<D> &rw) {
-        constexpr int N = NV<D>::value;
-        constexpr int NE = 2 * D + D * D + 1;
-        static_assert(sizeof(State<D>) == N * sizeof(double), "State<D> must be a plain array of doubles");
+        constexpr int N = NVS<D>::value;
+        constexpr int NE = 2 * D + SState<D>::S + 1;  // complex entries carried
+        constexpr int NE_FULL = 2 * D + D * D + 1;     // entries of the full state (the norm's count)
+        static_assert(sizeof(SState<D>) == N * sizeof(double), "SState<D> must be a plain array of doubles");
         if (k >= P.nt) return true;
         // Ending steps on the save times adds up to nt - 1 steps that an
         // integrator reading an interpolant would not take; they do not count
@@ -223,9 +345,9 @@ struct DopriBeam {
             hh = target - t;
             last = true;
         }
-        State<D> kk[7];
+        SState<D> kk[7];
         kk[0] = f0;
-        State<D> yt;
+        SState<D> yt;
         const double *yv = vals(y);
 #pragma unroll
         for (int s = 1; s < 7; ++s) {
@@ -239,7 +361,7 @@ struct DopriBeam {
                 }
                 tv[c] = yv[c] + hh * acc;
             }
-            rhs<D>(med, mode, yt, kk[s]);
+            rhs_sym<D>(med, mode, yt, kk[s]);
         }
         // yt now holds the 5th-order solution (stage 7's input).
         double sum = 0.0;
@@ -256,10 +378,10 @@ struct DopriBeam {
             for (int e = 0; e < NE; ++e) {
                 const double sc = o.atol + o.rtol * fmax(entry_abs<D>(yv, e), entry_abs<D>(nv, e));
                 const double r = entry_abs<D>(ev, e) / sc;
-                sum += r * r;
+                sum += sym_weight<D>(e) * (r * r);
             }
         }
-        const double err = sqrt(sum / NE);
+        const double err = sqrt(sum / NE_FULL);
         ++steps;
         if (!isfinite(err)) {
             h = 0.2 * hh;
@@ -273,10 +395,12 @@ struct DopriBeam {
             const double t_new = last ? target : t + hh;
             while (k < P.nt && P.ts[k] <= t_new) {
                 if (P.ts[k] == t_new) {
-                    rw.put(k, yt, false);
+                    State<D> yf;
+                    to_full(yt, yf);
+                    rw.put(k, yf, false);
                 } else {
                     const double th = (P.ts[k] - t) / hh;
-                    State<D> yd;
+                    SState<D> yd;
                     double *dv = vals(yd);
 #pragma unroll
                     for (int c = 0; c < N; ++c) {
@@ -291,7 +415,9 @@ struct DopriBeam {
                         const double r4 = r2 - hh * vals(kk[6])[c] - r3;
                         dv[c] = yv[c] + th * (r2 + (1.0 - th) * (r3 + th * (r4 + (1.0 - th) * r5)));
                     }
-                    rw.put(k, yd, false);
+                    State<D> yf;
+                    to_full(yd, yf);
+                    rw.put(k, yf, false);
                 }
                 ++k;
             }
@@ -341,9 +467,11 @@ __global__ void dopri_kernel(ProbArgs P, MediumArgs med, BeamArgs B, TrajArgs T,
             while (bl < T.nb && o.only_flagged && T.status[bl] == 0) bl += stride;  // already accepted
             if (bl < T.nb) {
                 double mode, w;
-                launch_state<D>(B, T, bl, s.y, mode, w);
+                State<D> y0;
+                launch_state<D>(B, T, bl, y0, mode, w);
+                from_full(y0, s.y);
                 rw.reset(bl, w);
-                rw.put(0, s.y, false);
+                rw.put(0, y0, false);
                 s.init(med, P, o, mode);
                 active = true;
             }
@@ -354,7 +482,11 @@ __global__ void dopri_kernel(ProbArgs P, MediumArgs med, BeamArgs B, TrajArgs T,
 #pragma unroll
             for (int i = 0; i < D; ++i) fin = fin && isfinite(s.y.x[i]) && isfinite(s.y.p[i]);
             if (!fin && s.code == 0) s.code = 1;
-            for (int64_t k = s.k; k < P.nt; ++k) rw.put(k, s.y, true);  // after a failure: last state
+            if (s.k < P.nt) {  // after a failure: the last state
+                State<D> yf;
+                to_full(s.y, yf);
+                for (int64_t k = s.k; k < P.nt; ++k) rw.put(k, yf, true);
+            }
             if (T.status) T.status[bl] = s.code;
             active = false;
         }
@@ -419,8 +551,8 @@ __global__ void tr_final_kernel(ProbArgs P, MediumArgs med, TrBeamsView B, int64
         s.y.x[a] = B.x[i * D + a];
         s.y.p[a] = B.p[i * D + a];
 #pragma unroll
-        for (int b = 0; b < D; ++b)
-            s.y.M[a][b] = cd{B.M[2 * ((i * D + a) * D + b)], B.M[2 * ((i * D + a) * D + b) + 1]};
+        for (int b = a; b < D; ++b)
+            s.y.M[sym_index<D>(a, b)] = cd{B.M[2 * ((i * D + a) * D + b)], B.M[2 * ((i * D + a) * D + b) + 1]};
     }
     s.y.A = cd{1.0, 0.0};
     const double t0 = B.t0[i];
@@ -442,7 +574,9 @@ __global__ void tr_final_kernel(ProbArgs P, MediumArgs med, TrBeamsView B, int64
     for (int a = 0; a < D; ++a) fin = fin && isfinite(s.y.x[a]) && isfinite(s.y.p[a]);
     if (!fin && code == 0) code = 1;
     double *r = rec64 + i * (int64_t)NV<D>::value;
-    const double *v = vals(s.y);
+    State<D> yf;
+    to_full(s.y, yf);
+    const double *v = vals(yf);
 #pragma unroll
     for (int c = 0; c < NV<D>::value; ++c) r[c] = v[c];
     status[i] = code;
