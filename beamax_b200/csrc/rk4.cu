@@ -136,21 +136,23 @@ __device__ __forceinline__ void from_full(const State<D> &f, SState<D> &s) {
 
 // coupled_rhs_absorption on the symmetric state (the same terms as rhs; dM
 // is formed for i <= k only).
-template <int D>
+// (The reciprocals 1/|p| and 1/|p|^3 replace FP64 divisions.)
+template <int D, int KIND>
 __device__ void rhs_sym(const MediumArgs &med, double mode, const SState<D> &y, SState<D> &dy) {
     double c, gc[D], hc[D * D];
-    speed_eval<D>(med, y.x, c, gc, hc);
+    speed_eval_k<D, KIND>(med, y.x, c, gc, hc);
     double n2 = 0.0;
 #pragma unroll
     for (int i = 0; i < D; ++i) n2 += y.p[i] * y.p[i];
     const double np = sqrt(n2);
-    const double np3 = np * n2;
+    const double inp = 1.0 / np;
+    const double inp3 = inp * inp * inp;
     const double G = mode * c * np;
     double Gx[D], Gp[D];
 #pragma unroll
     for (int i = 0; i < D; ++i) {
         Gx[i] = mode * gc[i] * np;
-        Gp[i] = mode * c * y.p[i] / np;
+        Gp[i] = mode * c * y.p[i] * inp;
         dy.x[i] = Gp[i];
         dy.p[i] = -Gx[i];
     }
@@ -159,8 +161,8 @@ __device__ void rhs_sym(const MediumArgs &med, double mode, const SState<D> &y, 
     for (int i = 0; i < D; ++i)
 #pragma unroll
         for (int k = 0; k < D; ++k) {
-            Gpp[i][k] = mode * c * ((i == k ? 1.0 / np : 0.0) - y.p[i] * y.p[k] / np3);
-            Gxp[i][k] = mode * gc[i] * y.p[k] / np;
+            Gpp[i][k] = mode * c * ((i == k ? inp : 0.0) - y.p[i] * y.p[k] * inp3);
+            Gxp[i][k] = mode * gc[i] * y.p[k] * inp;
         }
     cd MG[D][D];
 #pragma unroll
@@ -303,7 +305,7 @@ __constant__ double DP_D[7] = {-12715105075.0 / 11282082432.0, 0.0, 87487479700.
 //   1: steps follow the error control alone (only the last is shortened to
 //      end at ts[nt-1]) and save times inside a step are read from the
 //      continuous extension, as diffrax's SaveAt(ts) reads its interpolant.
-template <int D>
+template <int D, int KIND>
 struct DopriBeam {
     SState<D> y, f0;
     double t, h, mode;
@@ -319,7 +321,7 @@ struct DopriBeam {
         k = 1;
         rejected = false;
         code = 0;
-        rhs_sym<D>(med, mode, y, f0);
+        rhs_sym<D, KIND>(med, mode, y, f0);
     }
 
     // One attempt; returns true when the beam is finished (all save times
@@ -361,7 +363,7 @@ struct DopriBeam {
                 }
                 tv[c] = yv[c] + hh * acc;
             }
-            rhs_sym<D>(med, mode, yt, kk[s]);
+            rhs_sym<D, KIND>(med, mode, yt, kk[s]);
         }
         // yt now holds the 5th-order solution (stage 7's input).
         double sum = 0.0;
@@ -454,12 +456,12 @@ __device__ void launch_state(const BeamArgs &B, const TrajArgs &T, int64_t bl, S
 // i, i + stride, i + 2 stride, ... one attempted step per loop trip, so a
 // lane whose beam finishes early starts its next beam instead of idling
 // until the slowest beam of its warp is done.
-template <int D>
+template <int D, int KIND>
 __global__ void dopri_kernel(ProbArgs P, MediumArgs med, BeamArgs B, TrajArgs T, OdeArgs o, int tt_len) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     int64_t bl = blockIdx.x * (int64_t)blockDim.x + threadIdx.x - stride;
     bool active = false;
-    DopriBeam<D> s;
+    DopriBeam<D, KIND> s;
     RecordWriter<D> rw(P, T, 0, 0.0, tt_len);
     for (;;) {
         if (!active) {
@@ -540,12 +542,12 @@ struct TrBeamsView {
     const double *x, *p, *M, *mode, *t0;
 };
 
-template <int D>
+template <int D, int KIND>
 __global__ void tr_final_kernel(ProbArgs P, MediumArgs med, TrBeamsView B, int64_t n, OdeArgs o, double *rec64,
                                 int32_t *status) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
-    DopriBeam<D> s;
+    DopriBeam<D, KIND> s;
 #pragma unroll
     for (int a = 0; a < D; ++a) {
         s.y.x[a] = B.x[i * D + a];
@@ -580,6 +582,25 @@ __global__ void tr_final_kernel(ProbArgs P, MediumArgs med, TrBeamsView B, int64
 #pragma unroll
     for (int c = 0; c < NV<D>::value; ++c) r[c] = v[c];
     status[i] = code;
+}
+
+// The integrator kernels specialised for the medium kind (run-time kind ->
+// template argument).
+struct Dopri {
+    template <int D, int K>
+    static auto kernel() { return dopri_kernel<D, K>; }
+};
+struct TrFinal {
+    template <int D, int K>
+    static auto kernel() { return tr_final_kernel<D, K>; }
+};
+template <int D, typename Launch, typename Which>
+void launch_by_kind(int kind, Launch launch, Which) {
+    switch (kind) {
+        case MSGB_MEDIUM_CONSTANT: launch(Which::template kernel<D, MSGB_MEDIUM_CONSTANT>()); break;
+        case MSGB_MEDIUM_LINEAR: launch(Which::template kernel<D, MSGB_MEDIUM_LINEAR>()); break;
+        default: launch(Which::template kernel<D, MSGB_MEDIUM_BSPLINE3>()); break;
+    }
 }
 
 }  // namespace
@@ -618,9 +639,12 @@ extern "C" int msgb_tr_final_states(const msgb_problem *prob, const msgb_medium 
     const unsigned grid = (unsigned)((beams->n + blk - 1) / blk);
     cudaStream_t st = as_stream(stream);
     switch (prob->ndim) {
-        case 1: tr_final_kernel<1><<<grid, blk, 0, st>>>(P, M, B, beams->n, O, rec64, status); break;
-        case 2: tr_final_kernel<2><<<grid, blk, 0, st>>>(P, M, B, beams->n, O, rec64, status); break;
-        default: tr_final_kernel<3><<<grid, blk, 0, st>>>(P, M, B, beams->n, O, rec64, status); break;
+        case 1: launch_by_kind<1>(M.kind, [&](auto kern) { kern<<<grid, blk, 0, st>>>(P, M, B, beams->n, O, rec64, status); },
+                                  TrFinal{}); break;
+        case 2: launch_by_kind<2>(M.kind, [&](auto kern) { kern<<<grid, blk, 0, st>>>(P, M, B, beams->n, O, rec64, status); },
+                                  TrFinal{}); break;
+        default: launch_by_kind<3>(M.kind, [&](auto kern) { kern<<<grid, blk, 0, st>>>(P, M, B, beams->n, O, rec64, status); },
+                                   TrFinal{}); break;
     }
     return check_launch("msgb_tr_final_states");
 }
@@ -671,9 +695,12 @@ extern "C" int msgb_ode_trajectories(const msgb_problem *prob, const msgb_medium
         const int64_t want = 4LL * sms;
         const unsigned grid = (unsigned)(need < want ? need : want);
         switch (prob->ndim) {
-            case 1: dopri_kernel<1><<<grid, blk, 0, st>>>(P, M, to_args(beams), T, O, MSGB_TIME_TILE); break;
-            case 2: dopri_kernel<2><<<grid, blk, 0, st>>>(P, M, to_args(beams), T, O, MSGB_TIME_TILE); break;
-            default: dopri_kernel<3><<<grid, blk, 0, st>>>(P, M, to_args(beams), T, O, MSGB_TIME_TILE); break;
+            case 1: launch_by_kind<1>(M.kind, [&](auto kern) { kern<<<grid, blk, 0, st>>>(P, M, to_args(beams), T, O, MSGB_TIME_TILE); },
+                                      Dopri{}); break;
+            case 2: launch_by_kind<2>(M.kind, [&](auto kern) { kern<<<grid, blk, 0, st>>>(P, M, to_args(beams), T, O, MSGB_TIME_TILE); },
+                                      Dopri{}); break;
+            default: launch_by_kind<3>(M.kind, [&](auto kern) { kern<<<grid, blk, 0, st>>>(P, M, to_args(beams), T, O, MSGB_TIME_TILE); },
+                                       Dopri{}); break;
         }
     }
     return check_launch("msgb_ode_trajectories");

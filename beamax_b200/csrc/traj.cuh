@@ -13,6 +13,7 @@ struct MediumArgs {
     int kind, boundary;
     int n[3];
     double spacing[3], origin[3];
+    double inv_spacing[3];  // 1 / spacing (multiplications instead of FP64 divisions)
     const double *coeffs;
     double c, lam;
 };
@@ -27,10 +28,11 @@ __device__ __forceinline__ int map_index(int i, int n, int boundary) {
     }
 }
 
-// c, grad c (D), hess c (D x D, row-major) at x.
-template <int D>
-__device__ void speed_eval(const MediumArgs &m, const double *x, double &c, double *g, double *H) {
-    if (m.kind == MSGB_MEDIUM_CONSTANT) {
+// c, grad c (D), hess c (D x D, row-major) at x, for a medium of kind KIND
+// (the tap count and the weights are then compile-time constants).
+template <int D, int KIND>
+__device__ __forceinline__ void speed_eval_k(const MediumArgs &m, const double *x, double &c, double *g, double *H) {
+    if (KIND == MSGB_MEDIUM_CONSTANT) {
         c = m.c;
 #pragma unroll
         for (int i = 0; i < D; ++i) {
@@ -40,14 +42,14 @@ __device__ void speed_eval(const MediumArgs &m, const double *x, double &c, doub
         }
         return;
     }
-    const bool cubic = m.kind == MSGB_MEDIUM_BSPLINE3;
-    const int taps = cubic ? 4 : 2;
-    const int off0 = cubic ? -1 : 0;
+    constexpr bool cubic = KIND == MSGB_MEDIUM_BSPLINE3;
+    constexpr int taps = cubic ? 4 : 2;
+    constexpr int off0 = cubic ? -1 : 0;
     double w[D][4], d1[D][4], d2[D][4];
     int idx[D][4];
 #pragma unroll
     for (int a = 0; a < D; ++a) {
-        const double u = (x[a] - m.origin[a]) / m.spacing[a];
+        const double u = (x[a] - m.origin[a]) * m.inv_spacing[a];
         const double fl = floor(u);
         const double t = u - fl;
         const int i0 = (int)fl;
@@ -73,6 +75,7 @@ __device__ void speed_eval(const MediumArgs &m, const double *x, double &c, doub
             d2[a][0] = d2[a][1] = 0.0;
             w[a][2] = w[a][3] = d1[a][2] = d1[a][3] = d2[a][2] = d2[a][3] = 0.0;
         }
+#pragma unroll
         for (int k = 0; k < taps; ++k) idx[a][k] = map_index(i0 + off0 + k, m.n[a], m.boundary);
     }
     // Separable reduction, last axis first: the tensor-product weights factor,
@@ -86,6 +89,7 @@ __device__ void speed_eval(const MediumArgs &m, const double *x, double &c, doub
         for (int k = 0; k < D; ++k) hh[i][k] = 0.0;
     }
     if (D == 1) {
+#pragma unroll
         for (int k = 0; k < taps; ++k) {
             const double v = __ldg(m.coeffs + idx[0][k]);
             cc = fma(w[0][k], v, cc);
@@ -94,9 +98,11 @@ __device__ void speed_eval(const MediumArgs &m, const double *x, double &c, doub
         }
     } else if (D == 2) {
         const int L = D - 1;  // last axis
+#pragma unroll
         for (int i = 0; i < taps; ++i) {
             const double *row = m.coeffs + (int64_t)idx[0][i] * m.n[L];
             double rw = 0.0, rd = 0.0, rdd = 0.0;
+#pragma unroll
             for (int k = 0; k < taps; ++k) {
                 const double v = __ldg(row + idx[L][k]);
                 rw = fma(w[L][k], v, rw);
@@ -112,11 +118,14 @@ __device__ void speed_eval(const MediumArgs &m, const double *x, double &c, doub
         }
     } else {
         const int Y = 1 % D, Z = 2 % D;
+#pragma unroll
         for (int i = 0; i < taps; ++i) {
             double tw = 0.0, ty = 0.0, tyy = 0.0, tz = 0.0, tyz = 0.0, tzz = 0.0;
+#pragma unroll
             for (int j = 0; j < taps; ++j) {
                 const double *line = m.coeffs + ((int64_t)idx[0][i] * m.n[Y] + idx[Y][j]) * m.n[Z];
                 double sw = 0.0, sd = 0.0, sdd = 0.0;
+#pragma unroll
                 for (int k = 0; k < taps; ++k) {
                     const double v = __ldg(line + idx[Z][k]);
                     sw = fma(w[Z][k], v, sw);
@@ -145,12 +154,22 @@ __device__ void speed_eval(const MediumArgs &m, const double *x, double &c, doub
     c = cc;
 #pragma unroll
     for (int a = 0; a < D; ++a) {
-        g[a] = gg[a] / m.spacing[a];
+        g[a] = gg[a] * m.inv_spacing[a];
 #pragma unroll
         for (int b = 0; b < D; ++b) {
             const double hv = a <= b ? hh[a][b] : hh[b][a];
-            H[a * D + b] = hv / (m.spacing[a] * m.spacing[b]);
+            H[a * D + b] = hv * (m.inv_spacing[a] * m.inv_spacing[b]);
         }
+    }
+}
+
+// The same for a medium kind known only at run time.
+template <int D>
+__device__ void speed_eval(const MediumArgs &m, const double *x, double &c, double *g, double *H) {
+    switch (m.kind) {
+        case MSGB_MEDIUM_CONSTANT: speed_eval_k<D, MSGB_MEDIUM_CONSTANT>(m, x, c, g, H); break;
+        case MSGB_MEDIUM_LINEAR: speed_eval_k<D, MSGB_MEDIUM_LINEAR>(m, x, c, g, H); break;
+        default: speed_eval_k<D, MSGB_MEDIUM_BSPLINE3>(m, x, c, g, H); break;
     }
 }
 
@@ -326,6 +345,7 @@ inline int medium_args(const msgb_problem *prob, const msgb_medium *med, MediumA
         M.spacing[a] = med->spacing[a];
         M.origin[a] = med->origin[a];
     }
+    for (int a = 0; a < 3; ++a) M.inv_spacing[a] = 1.0 / M.spacing[a];
     M.coeffs = med->coeffs;
     M.c = med->c;
     M.lam = med->lam;
