@@ -144,8 +144,10 @@ int msgb_sum_fwd_f32(const msgb_problem *prob, const msgb_beam_set *beams,
 int msgb_sum_fwd_f32_static(const msgb_problem *prob, const msgb_beam_set *beams,
                             const msgb_sum_opts *opts, float *out, msgb_stream_t stream);
 
-/* FP32 transpose of msgb_sum_fwd_f32 (same culling); one owner per beam, no
- * atomics.  data: (nt, ns) FP32.  g: (n) complex FP64. */
+/* FP32 transpose of msgb_sum_fwd_f32 (same culling), tile-parallel like the
+ * forward: per-beam partials are added to g with FP64 atomics, so results
+ * agree between runs to the last bits of FP64, not bit for bit.  data:
+ * (nt, ns) FP32.  g: (n) complex FP64, written by the call (zeroed first). */
 int msgb_adj_gather_f32(const msgb_problem *prob, const msgb_beam_set *beams,
                         const msgb_sum_opts *opts, void *workspace, size_t workspace_bytes,
                         const float *data, double *g, msgb_stream_t stream);
