@@ -780,7 +780,7 @@ fwd32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
 // and holds d(t, s) for its GS sensors in registers for the whole item.  Each
 // pair of surviving beams runs the forward's recurrence while the lane
 // accumulates sum_s d(t, s) conj(z(t, s)); the pair's partials are reduced
-// over the 32 times (FP64 shuffles, fixed order), over the warps (FP64, fixed
+// over the 32 times (FP32 shuffles, fixed order), over the warps (FP64, fixed
 // order) and added to the beam's FP64 slot with one atomic per (beam, item).
 // g must be zeroed first; the order of those atomic additions varies between
 // runs (last-bit differences of the FP64 result).
@@ -941,11 +941,16 @@ adj32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
                             }
                         }
                     }
-                    double v[4] = {(double)ar.x, (double)ai.x, (double)ar.y, (double)ai.y};
+                    // over the 32 times: paired FP32 adds (the partials are sums of
+                    // 16 terms; FP64 from here on)
 #pragma unroll
-                    for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-                        for (int c = 0; c < 4; ++c) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
+                    for (int o = 16; o > 0; o >>= 1) {
+                        ar = __fadd2_rn(ar, make_float2(__shfl_xor_sync(0xffffffffu, ar.x, o),
+                                                        __shfl_xor_sync(0xffffffffu, ar.y, o)));
+                        ai = __fadd2_rn(ai, make_float2(__shfl_xor_sync(0xffffffffu, ai.x, o),
+                                                        __shfl_xor_sync(0xffffffffu, ai.y, o)));
+                    }
+                    const double v[4] = {(double)ar.x, (double)ai.x, (double)ar.y, (double)ai.y};
                     if (lane == 0) {
                         part[warp][gl][0] = v[0];
                         part[warp][gl][1] = v[1];
