@@ -240,3 +240,20 @@ def test_reference_propagator_names_are_accepted():
                         (gs.solve_ODE_base, False)):
         s = bb.MSGBSolver(8, "top_n", 8, "spatial", ode, "scan_real", tr_ode_solver=gs.solve_hom_TR)
         assert s.closed_form is closed
+
+
+def test_bench_reports_the_dominant_summation_kernel():
+    """bench.py's roofline object is the summation kernel with the larger
+    device time, with its algorithmic flops per evaluated triple."""
+    import types
+
+    import bench
+
+    args = types.SimpleNamespace(thr=65536, workload="c2")
+    r = {"hetero": False, "fwd_evals": 8e10, "adj_evals": 8e10, "t_fwd_kernel": 0.08, "t_adj_kernel": 0.09}
+    first, other = bench.summation_rooflines(r, 1965.0, args)
+    assert (first["kernel"], other["kernel"]) == ("adj32_kernel", "fwd32_kernel")
+    assert first["flops_per_eval"] == 40.0 and other["flops_per_eval"] == 36.0
+    assert abs(first["frac"] - 8e10 * 40 / 0.09 / 1e12 / (148 * 128 * 2 * 1965e6 / 1e12)) < 1e-12
+    r["t_fwd_kernel"] = 0.1
+    assert bench.summation_rooflines(r, 1965.0, args)[0]["kernel"] == "fwd32_kernel"
