@@ -126,9 +126,10 @@ class MSGBSolver:
         medium and time grid; heterogeneous beams are predicted by it and the
         ones it does not accept are integrated.
       keep_trajectories: in heterogeneous media, keep the last forward's
-        trajectory records on the device (when they fit in trajectory_memory)
-        so that an adjoint with the same selection, domain and time grid does
-        not integrate the beams again.
+        trajectory records on the device so that an adjoint with the same
+        selection, domain and time grid does not integrate those beams again:
+        all of them when they fit in trajectory_memory, else the last chunk
+        of beams (when the device has room for it beside the chunk buffer).
     """
 
     def __init__(self, thr, thr_strat: str, batch_size: int, input_type: str, ode_solver, sum_method: str,
@@ -517,13 +518,13 @@ class MSGBSolver:
         status = torch.zeros(2 * bt.n, dtype=torch.int32, device=dev)
         self._begin_trajectories(domain, ts)
         self._traj_cache = None
-        keep_buf = None
-        if self.keep_trajectories and self._traj_owner is not None and len(chunks) == 1:
-            keep_buf = torch.empty(per * chunks[0][1] + 4096, dtype=torch.uint8, device=dev)
+        keep_buf = self._keep_buffer(chunks, per, dev)
+        last = len(chunks) - 1
         if fp64:
             out = torch.zeros((pr.nt, pr.ns), dtype=torch.float64, device=dev)
-            for b_first, nb in chunks:
-                tr, buf = self._trajectories(pr, med, bs, b_first, nb, True, per, n_tt, dev, st, status, keep_buf)
+            for i, (b_first, nb) in enumerate(chunks):
+                tr, buf = self._trajectories(pr, med, bs, b_first, nb, True, per, n_tt, dev, st, status,
+                                             keep_buf if i == last else None)
                 _lib.check(_lib.lib().msgb_sum_fwd_f64_traj(_lib.ref(pr), _lib.ref(bs), _lib.ref(tr), out.data_ptr(),
                                                             st), "msgb_sum_fwd_f64_traj")
             self._check_status(status)
@@ -537,7 +538,8 @@ class MSGBSolver:
         nbytes = _lib.lib().msgb_sum_f32_traj_workspace_size(_lib.ref(pr), 2 * bt.n)
         ws = workspace(dev, "sum32traj", nbytes)
         for i, (b_first, nb) in enumerate(chunks):
-            tr, buf = self._trajectories(pr, med, bs, b_first, nb, False, per, n_tt, dev, st, status, keep_buf)
+            tr, buf = self._trajectories(pr, med, bs, b_first, nb, False, per, n_tt, dev, st, status,
+                                         keep_buf if i == last else None)
             with self._kernel_span("msgb_sum_fwd_f32_traj", cnt):
                 _lib.check(_lib.lib().msgb_sum_fwd_f32_traj(_lib.ref(pr), _lib.ref(bs), _lib.ref(tr), _lib.ref(opts),
                                                             int(i == 0), int(i == len(chunks) - 1), ws.data_ptr(),
@@ -546,6 +548,23 @@ class MSGBSolver:
         self._check_status(status)
         self._remember_trajectories(keep_buf, tr, domain, ts, pr.nt)
         return out
+
+    def _keep_buffer(self, chunks, per, dev):
+        """Own memory for the records of the forward's last chunk of beams, so
+        that an adjoint with the same selection reads them instead of
+        integrating those beams again.  One chunk: the whole step integrates
+        once.  Several chunks (records larger than trajectory_memory): the
+        last chunk is kept when the device has room for a second buffer."""
+        import torch
+
+        if not self.keep_trajectories or self._traj_owner is None:
+            return None
+        size = per * chunks[-1][1] + 4096
+        if len(chunks) > 1:
+            free, _ = torch.cuda.mem_get_info(dev)
+            if free < size + (4 << 30):
+                return None
+        return torch.empty(size, dtype=torch.uint8, device=dev)
 
     def _remember_trajectories(self, buf, tr, domain, ts, nt):
         if buf is None:
@@ -587,10 +606,9 @@ class MSGBSolver:
         ws = None if fp64 else workspace(dev, "sum32traj", nbytes)
         status = torch.zeros(2 * n, dtype=torch.int32, device=dev)
         self._begin_trajectories(domain, ts)
-        if cached is not None:
-            chunks = [(0, 2 * n)]
+        kept = (cached["tr"].b_first, cached["tr"].nb) if cached is not None else None
         for b_first, nb in chunks:
-            if cached is not None:
+            if (b_first, nb) == kept:
                 tr = cached["tr"]  # the forward's records for these beams, in this order
             else:
                 tr, _ = self._trajectories(pr, med, bs, b_first, nb, fp64, per, n_tt, dev, st, status)

@@ -361,6 +361,29 @@ def test_adjoint_reuses_forward_trajectories():
         assert om.rel_l2(a_fresh, a_keep) < (1e-12 if precision == "fp64" else 1e-6)
 
 
+def test_adjoint_reuses_the_last_chunk_of_forward_trajectories():
+    """Records larger than trajectory_memory are integrated in chunks; the
+    adjoint reads the kept last chunk and integrates the others, with the
+    result of the adjoint that integrates every chunk."""
+    import beamax_b200 as bb
+
+    _dev()
+    dom, wpt, p0, sens, ts, c, interp, thr = _het_case(seed=2, N=(64, 64), thr=60)
+    ode = bb.gb.gb_solvers.solve_ODE_base
+    for precision in ("fp64", "fp32"):
+        kw = dict(precision=precision, trajectory_memory=256 << 10)
+        keep = bb.MSGBSolver(thr, "top_n", 64, "spatial", ode, "scan_real", **kw)
+        fresh = bb.MSGBSolver(thr, "top_n", 64, "spatial", ode, "scan_real", keep_trajectories=False, **kw)
+        y = keep.forward(p0, dom, sens, ts, wpt)
+        fresh.forward(p0, dom, sens, ts, wpt)
+        cached = keep._cached_trajectories(keep.last_selection, dom, ts)
+        assert cached is not None and 0 < cached["tr"].nb < 2 * keep.last_selection.idx.shape[0]
+        data = np.random.default_rng(9).standard_normal(y.shape)
+        a_keep = keep.adjoint(data, dom, sens, ts, wpt)
+        a_fresh = fresh.adjoint(data, dom, sens, ts, wpt)
+        assert om.rel_l2(a_fresh, a_keep) < (1e-12 if precision == "fp64" else 1e-6)
+
+
 def _het3d_case(thr):
     import beamax_b200 as bb
 
