@@ -924,6 +924,24 @@ class MSGBSolver:
             raise ValueError("sources must form a complete Cartesian detector grid.")
 
     @staticmethod
+    def _infer_planar_surface(sensor_positions, eps: float = 1e-9):
+        """msgb_solver.py:755-805: the detector plane x_axis = coord of sensor
+        positions (the axis of smallest spread, which must be below eps) and
+        its implicit function x -> x[axis] - coord."""
+        pos = np.asarray(sensor_positions.detach().cpu().numpy() if hasattr(sensor_positions, "detach")
+                         else sensor_positions, dtype=np.float64)
+        stds = np.std(pos, axis=0)
+        axis = int(np.argmin(stds))
+        if stds[axis] > eps:
+            raise ValueError("Cannot infer planar surface from sensor positions; please provide `surface`.")
+        coord = float(pos[0, axis])
+
+        def surface(x):
+            return np.asarray(x, dtype=np.float64)[..., axis] - coord
+
+        return surface, axis, coord
+
+    @staticmethod
     def _tr_geometry(sources: Sensor) -> _lib.TrGeometry:
         """The detector plane (tr_solver_utils.py:173-204, 241-251, 377-393):
         the first constant column of the source positions is the normal axis

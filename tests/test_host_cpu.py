@@ -257,3 +257,26 @@ def test_bench_reports_the_dominant_summation_kernel():
     assert abs(first["frac"] - 8e10 * 40 / 0.09 / 1e12 / (148 * 128 * 2 * 1965e6 / 1e12)) < 1e-12
     r["t_fwd_kernel"] = 0.1
     assert bench.summation_rooflines(r, 1965.0, args)[0]["kernel"] == "fwd32_kernel"
+
+
+def test_infer_planar_surface_matches_reference():
+    """MSGBSolver._infer_planar_surface (tests/solvers/test_msgb_solver_misc.py:
+    116-141): axis, coordinate and implicit function of a planar detector;
+    generic positions are rejected."""
+    s = bb.MSGBSolver(4, "top_n", 4, "spatial", "solve_hom_diag", "all_real")
+    y = np.linspace(0.0, 1.0, 5)
+    surface, axis, coord = s._infer_planar_surface(np.stack([np.full_like(y, 2.0), y], 1))
+    assert axis == 0 and coord == pytest.approx(2.0)
+    assert float(surface(np.array([2.0, 0.5]))) == pytest.approx(0.0)
+    assert float(surface(np.array([3.0, 0.5]))) == pytest.approx(1.0)
+    with pytest.raises(ValueError, match="planar surface"):
+        s._infer_planar_surface(np.array([[0.0, 0.0], [1.0, 0.5], [0.3, 0.8], [0.7, 0.2]]))
+
+
+def test_forward_rejects_unsupported_sensor_type():
+    """tests/solvers/test_msgb_solver_misc.py:160-166."""
+    dom = bb.Domain(N=(128,), dx=(1.0 / 128,), periodic=(False,), c=1.0)
+    wpt = bb.MSWPT(bb.DyadicDecomposition(2, (128,), (4, 8), (1,)), 2, "rectangular")
+    s = bb.MSGBSolver(4, "top_n", 4, "spatial", "solve_hom_diag", "all_real")
+    with pytest.raises(ValueError, match="Unsupported sensor type"):
+        s.forward(np.zeros(dom.N), dom, "not_a_sensor", np.linspace(0.0, 1.0, 8), wpt)
