@@ -280,3 +280,16 @@ def test_forward_rejects_unsupported_sensor_type():
     s = bb.MSGBSolver(4, "top_n", 4, "spatial", "solve_hom_diag", "all_real")
     with pytest.raises(ValueError, match="Unsupported sensor type"):
         s.forward(np.zeros(dom.N), dom, "not_a_sensor", np.linspace(0.0, 1.0, 8), wpt)
+
+
+@pytest.mark.parametrize("threshold,strategy,match", [
+    (0, "top_n", "positive integer"),
+    (1.5, "top_n", "positive integer"),
+    (-1.0, "hard", "non-negative"),
+    (101.0, "percentile", r"\[0, 100\]"),
+    (1.1, "perc_max_abs", r"\[0, 1\]"),
+])
+def test_threshold_configuration_is_validated(threshold, strategy, match):
+    """tests/solvers/test_msgb_solver_misc.py:424-446."""
+    with pytest.raises(ValueError, match=match):
+        bb.MSGBSolver(threshold, strategy, 4, "spatial", bb.gb.gb_solvers.solve_ODE_base, "all_real")
