@@ -59,7 +59,7 @@ class Medium(ctypes.Structure):
 
 class OdeOpts(ctypes.Structure):
     _fields_ = [("method", c_i32), ("substeps", c_i32), ("rtol", c_dbl), ("atol", c_dbl), ("dt0", c_dbl),
-                ("max_steps", c_i64), ("only_flagged", c_i32), ("dense_output", c_i32)]
+                ("max_steps", c_i64), ("only_flagged", c_i32), ("dense_output", c_i32), ("step_count", c_vp)]
 
 
 class SurrogateIO(ctypes.Structure):
@@ -145,6 +145,8 @@ SIGNATURES = {
     "msgb_tr_final_states": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "msgb_scatter_coeff_grad": (ctypes.c_int, [c_vp, c_vp, c_i64, c_dbl, c_vp, ctypes.c_int,
                                                 c_vp, c_vp]),
+    "msgb_peak_probe_ops": (c_dbl, [ctypes.c_int, c_i64, ctypes.c_int, ctypes.c_int]),
+    "msgb_peak_probe": (ctypes.c_int, [ctypes.c_int, c_i64, ctypes.c_int, ctypes.c_int, c_vp, c_vp]),
 }
 
 _lock = threading.Lock()

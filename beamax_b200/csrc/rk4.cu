@@ -250,6 +250,7 @@ struct OdeArgs {
     double rtol, atol, dt0;
     int64_t max_steps;
     int only_flagged, dense_output;
+    unsigned long long *step_count;  // optional: attempted steps are added to it
 };
 
 template <int D>
@@ -496,6 +497,7 @@ __global__ void dopri_kernel(ProbArgs P, MediumArgs med, BeamArgs B, TrajArgs T,
     s.ks = dopri_stage_smem + threadIdx.x;
     s.kst = blockDim.x;
     RecordWriter<D> rw(P, T, 0, 0.0, tt_len);
+    unsigned long long lane_steps = 0;
     for (;;) {
         if (!active) {
             bl += stride;
@@ -523,8 +525,14 @@ __global__ void dopri_kernel(ProbArgs P, MediumArgs med, BeamArgs B, TrajArgs T,
                 for (int64_t k = s.k; k < P.nt; ++k) rw.put(k, yf, true);
             }
             if (T.status) T.status[bl] = s.code;
+            lane_steps += (unsigned long long)s.steps;
             active = false;
         }
+    }
+    if (o.step_count) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) lane_steps += __shfl_xor_sync(0xffffffffu, lane_steps, off);
+        if ((threadIdx.x & 31) == 0 && lane_steps) atomicAdd(o.step_count, lane_steps);
     }
 }
 
@@ -673,7 +681,7 @@ extern "C" int msgb_tr_final_states(const msgb_problem *prob, const msgb_medium 
     }
     P.c = prob->c;
     OdeArgs O{opts->method, opts->substeps, opts->rtol, opts->atol, opts->dt0, opts->max_steps, 0,
-              opts->dense_output};
+              opts->dense_output, nullptr};
     TrBeamsView B{beams->x, beams->p, beams->M, beams->mode, beams->t0};
     const int blk = 64;
     const unsigned grid = (unsigned)((beams->n + blk - 1) / blk);
@@ -715,7 +723,7 @@ extern "C" int msgb_ode_trajectories(const msgb_problem *prob, const msgb_medium
         return fail(MSGB_ERR_ARG, "only_flagged needs the status array of the records");
     ProbArgs P = to_args(prob);
     OdeArgs O{opts->method, opts->substeps, opts->rtol, opts->atol, opts->dt0, opts->max_steps, opts->only_flagged,
-              opts->dense_output};
+              opts->dense_output, opts->step_count};
     TrajArgs T{out->nb, out->b_first, beams->n, out->rec64, out->rec32, out->cull, out->status};
     const int blk = 64;
     const int64_t need = (out->nb + blk - 1) / blk;

@@ -202,6 +202,9 @@ class MSGBSolver:
         # (name, start event, end event, evaluation counter) recorded on the
         # launching stream around the call.
         self.kernel_timer = None
+        # When set to a one-element int64 CUDA tensor, the adaptive ODE adds the
+        # number of attempted steps (accepted + rejected) of every integration to it.
+        self.ode_step_counter = None
         self.last_surrogate_accepted: Optional[int] = None
         self._accepted = None
         self.last_selection: Optional[Selection] = None
@@ -462,6 +465,8 @@ class MSGBSolver:
                                cull=None if fp64 else base + cull_off,
                                status=status.data_ptr() + 4 * b_first)
         opts = self._ode_opts(None)
+        if self.ode_step_counter is not None:
+            opts.step_count = self.ode_step_counter.data_ptr()
         if self.surrogate is not None:
             self.surrogate.predict_into(pr, med, bs, b_first, nb, tr)
             acc = (status[b_first:b_first + nb] == 0).sum()

@@ -1,31 +1,33 @@
 #!/usr/bin/env python
-"""Benchmark: MSGB forward + exact adjoint on one B200 (beamax config 2).
+"""Benchmark: MSGB forward + exact adjoint on one B200 (beamax config 3).
 
-Workload (the configuration the headline metric is quoted on that fits one
-GPU): 2D 512 x 512 grid, dx = 1e-4 m, homogeneous c = 1500 m/s, cfl 0.3
-(Nt = 2414); 4 levels, boxes (4, 8, 16, 32), redundancy 2,
-rectangular_mirror; p0 = 64 seeded Gaussian wave packets (centres in the inner
-80 %, directions uniform, |k| uniform in each level's annulus, amplitudes
-N(0, 1)) + 8 Gaussian blobs (sigma 20 cells), max|p0| = 1; four-sided line
-sensor (2044 points); thr = 65536 top_n (131072 beams); solve_hom_diag.
-Synthetic data of those shapes; nothing is downloaded.
+Default workload (``--workload c3``; the configuration the headline metric
+is quoted on, and it fits one GPU): 2D 1024 x 1024 grid, dx = 5e-5 m,
+c(x) = 1500 (1 + 0.08 g(x)) with g a seeded Gaussian random field of 40-cell
+correlation length clipped to [-1, 1] (cubic B-spline interpolant), cfl 0.3
+(Nt ~ 5,600); 4 levels, boxes (4, 8, 16, 32), redundancy 2,
+rectangular_mirror (the stated 5-level tiling is rejected by the reference's
+own validation); p0 = 256 seeded Gaussian wave packets + 8 blobs, max|p0| = 1;
+four-sided line sensor (4092 points); thr = 262144 top_n (524288 beams);
+adaptive FP64 beam ODE (Dormand-Prince 5(4), rtol 1e-7, atol 1e-9).
+Synthetic seeded data of those shapes; nothing is downloaded.
 
 A step = one forward (p0 -> sensor data) plus one exact adjoint (data ->
-image) on the FP32 path (Kahan sums, FP64 anchor phases, Gaussian cutoff).
-The dense FP64 path (reference semantics) is run once for comparison and as
-the accuracy reference.  ``value`` = dense-equivalent beam-sample evaluations
-per second of forward + adjoint (2 * 2n * Nt * Ns per step / step time).
+image) on the FP32 path (Kahan sums, FP64 anchor phases, Gaussian cutoff;
+beams integrated by the FP64 ODE).  The dense FP64 path (reference
+semantics: every beam at every time and sensor) is run once for comparison
+and as the accuracy reference.  ``value`` = dense-equivalent beam-sample
+evaluations per second of forward + adjoint (2 * 2n * Nt * Ns per step / step
+time).
 
 ``--impl reference`` times the CPU restatement of the reference algorithm
-(C/OpenMP FP64, dense, all host threads) on a bounded beam sample and
-reports the same metric.
+(C/OpenMP FP64, dense, all host threads: for heterogeneous workloads the
+adaptive beam ODE plus the dense trajectory sums) on a bounded sample of the
+selected beams and reports the same metric.
 
-``--workload het512`` / ``c3`` / ``c5`` measure the heterogeneous path instead
-(seeded random sound speed, adaptive FP64 beam ODE, trajectory summation):
-het512 is config 2's geometry in a 20-cell-correlation medium, c3 the 1024^2,
-dx 5e-5, 40-cell-correlation configuration with the valid 4-level tiling and
-thr 262,144, c5 the 3D 128^3 configuration (their dense FP64 comparisons take
-minutes).
+``--workload c2`` (512^2 homogeneous, four-sided sensor, thr 65,536),
+``het512`` (config 2's geometry in a 20-cell-correlation medium) and ``c5``
+(3D 128^3) measure the other configurations.
 """
 
 from __future__ import annotations
@@ -226,6 +228,56 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+# ---------------------------------------------------------------- peaks
+def measure_peaks(device):
+    """FP32 (scalar FFMA and paired FFMA2), FP64 (DFMA) and MUFU throughput of
+    this GPU with libmsgb's probe kernels (8 blocks of 256 threads per SM, 8
+    independent chains per thread), each timed with CUDA events after one
+    warm-up launch.  TFLOP/s (FMA = 2 flops) or, for MUFU, Tops/s."""
+    import torch
+
+    from beamax_b200 import _lib
+
+    L = _lib.lib()
+    props = torch.cuda.get_device_properties(device)
+    blocks, threads = props.multi_processor_count * 8, 256
+    sink = torch.empty(blocks * threads, dtype=torch.float32, device=device)
+    st = torch.cuda.current_stream(device)
+    out = {}
+    for name, kind, iters in (("fp32", 0, 200000), ("fp32x2", 1, 100000), ("fp64", 2, 100000), ("mufu", 3, 20000)):
+        _lib.check(L.msgb_peak_probe(kind, 1000, blocks, threads, sink.data_ptr(), st.cuda_stream), "probe")
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        _lib.check(L.msgb_peak_probe(kind, iters, blocks, threads, sink.data_ptr(), st.cuda_stream), "probe")
+        b.record(st)
+        torch.cuda.synchronize(device)
+        secs = a.elapsed_time(b) / 1e3
+        out[name] = L.msgb_peak_probe_ops(kind, iters, blocks, threads) / secs / 1e12
+    out["fp32_best"] = max(out["fp32"], out["fp32x2"])
+    out["method"] = (f"msgb_peak_probe: {blocks} blocks x {threads} threads, 8 independent chains of FFMA / FFMA2 / "
+                     "DFMA / MUFU.SIN per thread, CUDA events, after one warm-up launch; FMA = 2 flops")
+    return out
+
+
+def ode_flops_per_step(d: int) -> float:
+    """Algorithmic FP64 flops of one attempted Dormand-Prince step of the beam
+    ODE in a cubic B-spline medium (add, multiply, divide, square root, power
+    = 1 flop; FMA = 2), counted from the operations of the formulas:
+      * c, grad c, Hessian c at a point: per axis the B-spline weights and
+        their first and second derivatives (36 flops), then the separable
+        tensor-product sums: 2D 4 x 4 x 3 + 4 x 6 FMA, 3D 4^3 x 3 + 16 x 6 +
+        4 x 10 FMA, and the 1/spacing scaling: 226 (2D) / 785 (3D);
+      * coupled_rhs_absorption on the symmetric Riccati state (G, G_x, G_p,
+        G_pp, G_xp, M G_pp, the d(d+1)/2 entries of dM = -(G_xx + G_xp M +
+        M G_xp^T + M G_pp M), tr M, G_p^T M G_p and dA): 228 (2D) / 578 (3D);
+      * per step: 6 right-hand sides (first same as last), the 20 nonzero
+        stage coefficients and 6 stage inputs over the N = 12 (2D) / 20 (3D)
+        real state entries, the 7-term error estimate and the RMS error norm
+        with |.| of each complex entry: 900 (2D) / 1494 (3D).
+    2D: 6 x 454 + 900 = 3624; 3D: 6 x 1363 + 1494 = 9672."""
+    return {2: 3624.0, 3: 9672.0}.get(d, 3624.0)
+
+
 # ---------------------------------------------------------------- ours
 def launches_per_step(levels: int) -> int:
     """Kernels of libmsgb launched per step (cuFFT's own kernels excluded)."""
@@ -274,6 +326,8 @@ def run_ours(args, rank, world, device):
         sampler.start()
     times = []
     s32.kernel_timer = []  # events around each summation entry point, inside the timed steps
+    steps_ctr = torch.zeros(1, dtype=torch.int64, device=device)
+    s32.ode_step_counter = steps_ctr
     torch.cuda.synchronize()
     for _ in range(args.steps):
         flush.zero_()
@@ -287,6 +341,8 @@ def run_ours(args, rank, world, device):
         torch.distributed.barrier()
     spans = s32.kernel_timer
     s32.kernel_timer = None
+    s32.ode_step_counter = None
+    ode_steps = int(steps_ctr.item()) / args.steps
 
     def span_time(name):
         """Device time per step of every call of one entry point (all chunks)."""
@@ -324,7 +380,8 @@ def run_ours(args, rank, world, device):
     e2e_t = float(np.mean(e2e))
 
     result = {"rank": rank, "t_step": total / args.steps, "t_fwd_kernel": t_fwd_kernel, "t_adj_kernel": t_adj_kernel,
-              "t_ode": t_ode, "hetero": W["hetero"],
+              "t_ode": t_ode, "ode_steps": ode_steps, "ndim": len(dom.N), "hetero": W["hetero"],
+              "nt": nt, "ns": ns, "n_beams": 2 * n,
               # heterogeneous: one ODE and one summation call per trajectory chunk, each a prep + main kernel
               "extra_launches": 3 * sum(1 for nm, *_ in spans if "traj" in nm or "ode" in nm),
               "fwd_evals": fwd_evals, "adj_evals": adj_evals, "dense_step": dense_step, "clocks": clocks,
@@ -359,14 +416,23 @@ def run_ours(args, rank, world, device):
     return result
 
 
-def summation_rooflines(r, sm_mhz, args):
-    """FP32 rooflines of the two summation kernels, the one with the larger
-    device time per step first.  Algorithmic cost per evaluated (beam, time,
-    sensor) triple: 36 flops for the forward (24 FP32 instructions, FMA = 2),
-    40 for the transpose (+ 2 FMA for d conj(z)); peak = 148 SMs x 128 lanes x
-    2 flops x the median SM clock sampled under load.  DRAM traffic per launch
-    from the committed one-pass ncu capture of the config-2 workload."""
-    peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+def rooflines(r, peaks, sm_mhz, args):
+    """Rooflines of the step's kernels, the one with the largest device time
+    per step first (``roofline``), the others after it (``roofline_other``).
+
+    * Summation (``fwd32_kernel``, ``adj32_kernel``; ``<TRAJ>`` for the
+      trajectory variants): work unit = one evaluated (beam, time, sensor)
+      triple, 36 flops for the forward (24 FP32 instructions of a direct
+      evaluation, FMA = 2), 40 for the transpose (+ 2 FMA for d conj(z));
+      also the MUFU side (3 special-function operations per direct
+      evaluation).  Peak: the measured FP32 throughput (the better of FFMA and
+      FFMA2) and MUFU throughput of msgb_peak_probe.
+    * Beam ODE (``dopri_kernel``): attempted Dormand-Prince steps counted on the
+      device x ode_flops_per_step(d); peak: the measured DFMA throughput.
+    DRAM traffic per launch: the committed one-pass ncu capture for the
+    configuration-2 summation; null elsewhere (see profiles/)."""
+    fp32 = peaks["fp32_best"] if peaks else 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    basis32 = ("measured: " + peaks["method"]) if peaks else f"148 SM x 128 FP32 lanes x 2 x {sm_mhz:.0f} MHz"
     traffic = {}
     prof = os.path.join(ROOT, "profiles", "fwd32_traffic_config2.json")
     if os.path.exists(prof) and args.thr == 65536 and args.workload == "c2":
@@ -374,28 +440,53 @@ def summation_rooflines(r, sm_mhz, args):
             t = json.load(f)
         traffic = {"fwd": t.get("dram_bytes_per_launch"), "adj": t.get("adj32_dram_bytes_per_launch")}
     suffix = "<TRAJ>" if r["hetero"] else ""
-    out = {}
+    out = []
     for key, name, flops, evals, secs, what in (
             ("fwd", "fwd32_kernel", 36.0, r["fwd_evals"], r["t_fwd_kernel"], "forward summation"),
             ("adj", "adj32_kernel", 40.0, r["adj_evals"], r["t_adj_kernel"], "transpose gather")):
+        if secs <= 0:
+            continue
         achieved = evals * flops / secs / 1e12
-        out[key] = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                    "frac": achieved / peak, "traffic": traffic.get(key), "kernel": name + suffix,
-                    "flops_per_eval": flops, "device_s_per_step": secs,
-                    "peak_basis": f"148 SM x 128 FP32 lanes x 2 x {sm_mhz:.0f} MHz (median sampled SM clock)",
-                    "timing": f"CUDA events around the {what} entry point inside the timed steps "
-                              "(device time per step, all chunks)"}
-    first = "adj" if r["t_adj_kernel"] >= r["t_fwd_kernel"] else "fwd"
-    return out[first], out["fwd" if first == "adj" else "adj"]
+        entry = {"bound": "fp32", "achieved": achieved, "peak": fp32, "unit": "TFLOP/s",
+                 "frac": achieved / fp32, "traffic": traffic.get(key), "kernel": name + suffix,
+                 "flops_per_eval": flops, "device_s_per_step": secs, "peak_basis": basis32,
+                 "timing": f"CUDA events around the {what} entry point inside the timed steps "
+                           "(device time per step, all chunks)"}
+        if peaks:
+            mufu = 3.0 * evals / secs / 1e12
+            entry["mufu"] = {"achieved": mufu, "peak": peaks["mufu"], "unit": "Tops/s", "frac": mufu / peaks["mufu"],
+                             "ops_per_eval": 3}
+        out.append(entry)
+    if r["hetero"] and r["t_ode"] > 0 and r["ode_steps"] > 0:
+        fl = ode_flops_per_step(r["ndim"])
+        achieved = r["ode_steps"] * fl / r["t_ode"] / 1e12
+        peak = peaks["fp64"] if peaks else 148 * 64 * 2 * sm_mhz * 1e6 / 1e12
+        out.append({"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                    "traffic": None, "kernel": "dopri_kernel", "flops_per_step": fl,
+                    "attempted_steps_per_step": r["ode_steps"], "device_s_per_step": r["t_ode"],
+                    "peak_basis": ("measured: " + peaks["method"]) if peaks else
+                                  f"148 SM x 64 FP64 lanes x 2 x {sm_mhz:.0f} MHz",
+                    "timing": "CUDA events around every msgb_ode_trajectories call inside the timed steps; "
+                              "attempted steps counted on the device"})
+    out.sort(key=lambda e: -e["device_s_per_step"])
+    return out[0], out[1:]
 
 
-def cpu_reference(args, workload_only=False):
-    """Dense FP64 C/OpenMP restatement on a bounded beam sample (all host threads)."""
+CPU_SAMPLE = {"c2": 96, "het512": 64, "c3": 48, "c5": 32}
+
+
+def cpu_reference(args):
+    """Dense FP64 C/OpenMP restatement on a bounded sample of the selected
+    coefficients (both modes of each), all host threads.  Homogeneous media:
+    closed-form beams (oracle/csum.c); heterogeneous media: the adaptive
+    Dormand-Prince beam ODE, then the dense trajectory sums (oracle/chet.c).
+    The selection itself (MSWPT + top_n + beam init in the NumPy oracle) is
+    not timed; everything after it is."""
     import oracle.build as ob
     from oracle import msgb as om
 
     ob.build()
-    W = config2(seed=1234, thr=args.thr)
+    W = WORKLOADS[args.workload](seed=1234, thr=args.thr)
     dom, wpt, sens, ts, p0 = W["domain"], W["wpt"], W["sensors"], W["ts"], W["p0"]
     odom = om.Dom(N=dom.N, dx=dom.dx, periodic=dom.periodic, cfl=dom.cfl, c=1500.0)
     dec = wpt.dyadic_decomp
@@ -403,43 +494,63 @@ def cpu_reference(args, workload_only=False):
     t0 = time.perf_counter()
     bm = om.select_beams(p0, odom, ow, W["thr"])
     t_select = time.perf_counter() - t0
-    nsample = args.cpu_sample
+    nsample = args.cpu_sample or CPU_SAMPLE[args.workload]
     rng = np.random.default_rng(0)
     pick = np.sort(rng.choice(bm.idx.size, size=nsample, replace=False))
     sub = om.Beams(bm.idx[pick], bm.coeff[pick], bm.p0[pick], bm.M0[pick], bm.x0[pick], bm.omega[pick],
                    bm.a0_unit[pick])
     tab = om.beam_table(sub, 1500.0)
     pos = sens.positions
-    t0 = time.perf_counter()
-    y = ob.sum_hom(tab, 1500.0, ts, pos, dom.grid_size, dom.periodic)
-    t_fwd = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    ob.adj_hom(tab, sub.a0_unit, 1500.0, ts, pos, dom.grid_size, dom.periodic, y)
-    t_adj = time.perf_counter() - t0
+    t_ode = 0.0
+    if W["hetero"]:
+        cat = lambda a: np.concatenate([a, a])
+        mode = np.concatenate([np.ones(nsample), -np.ones(nsample)])
+        t0 = time.perf_counter()
+        rec, status, steps = ob.het_trajectories(cat(tab["x0"]), cat(tab["p0"]), cat(tab["alpha"]), mode,
+                                                 dom.medium()[1], ts)
+        t_ode = time.perf_counter() - t0
+        amp, om2 = cat(tab["a0"]), cat(tab["omega"])
+        t0 = time.perf_counter()
+        y = ob.sum_traj(rec, amp, om2, pos, dom.grid_size, dom.periodic)
+        t_fwd = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        ob.adj_traj(rec, om2, pos, dom.grid_size, dom.periodic, y)
+        t_adj = time.perf_counter() - t0
+        what = "adaptive Dormand-Prince beam ODE + dense FP64 trajectory sums, forward + exact adjoint (oracle/chet.c)"
+    else:
+        t0 = time.perf_counter()
+        y = ob.sum_hom(tab, 1500.0, ts, pos, dom.grid_size, dom.periodic)
+        t_fwd = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        ob.adj_hom(tab, sub.a0_unit, 1500.0, ts, pos, dom.grid_size, dom.periodic, y)
+        t_adj = time.perf_counter() - t0
+        what = "dense FP64 closed-form beams, forward + exact adjoint (oracle/csum.c)"
     evals = 2 * (2 * nsample) * ts.size * pos.shape[0]
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    value = evals / (t_fwd + t_adj)
-    full_s = (t_fwd + t_adj) * W["thr"] / nsample
+    t_all = t_ode + t_fwd + t_adj
+    value = evals / t_all
+    full_s = t_all * W["thr"] / nsample
     return {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": f"{nsample} of {W['thr']} selected coefficients ({2 * nsample} beams), all {ts.size} times x "
-                      f"{pos.shape[0]} sensors, dense FP64 forward + exact adjoint (C/OpenMP restatement); "
-                      f"full step extrapolated linearly in beams: {full_s:.1f} s",
-            "select_s": t_select, "t_fwd_s": t_fwd, "t_adj_s": t_adj, "workload": W["name"]}
+                      f"{pos.shape[0]} sensors; {what}, C/OpenMP on {cores} host threads; ODE {t_ode:.2f} s, "
+                      f"sums {t_fwd:.2f} + {t_adj:.2f} s; full step extrapolated linearly in beams: {full_s:.0f} s",
+            "select_s": t_select, "t_ode_s": t_ode, "t_fwd_s": t_fwd, "t_adj_s": t_adj, "workload": W["name"]}
 
 
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cutoff", type=float, default=16.0)
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2",
-                    help="c2: config 2 (the headline); het512 / c3 / c5: heterogeneous media")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c3",
+                    help="c3: config 3 (the headline); c2 / het512 / c5: the other configurations")
     ap.add_argument("--thr", type=int, default=None, help="top_n (default: the workload's; smaller for profiling)")
-    ap.add_argument("--cpu-sample", type=int, default=96)
+    ap.add_argument("--cpu-sample", type=int, default=None, help="coefficients timed by the CPU baseline")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-peaks", action="store_true")
     args = ap.parse_args()
     if args.thr is None:
         args.thr = DEFAULT_THR[args.workload]
@@ -450,10 +561,6 @@ def main():
 
     if args.impl == "reference":
         if rank != 0:
-            return 0
-        if args.workload != "c2":
-            print(json.dumps({"impl": "reference", "unavailable": "the CPU restatement of the summation covers "
-                              "homogeneous media (config 2); heterogeneous workloads have no CPU arm"}), flush=True)
             return 0
         r = cpu_reference(args)
         line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus,
@@ -472,13 +579,15 @@ def main():
 
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     device = torch.device("cuda", local_rank)
+    torch.cuda.set_device(device)
+    peaks = None if args.no_peaks else measure_peaks(device)
     r = run_ours(args, rank, world, device)
     if world > 1:
         torch.distributed.destroy_process_group()
     if rank != 0:
         return 0
     cpu = None
-    if not args.no_cpu_baseline and world == 1 and not r["hetero"]:
+    if not args.no_cpu_baseline and world == 1:
         try:
             cpu = cpu_reference(args)
             cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
@@ -488,12 +597,13 @@ def main():
     value = world * r["dense_step"] / t_step
     clk = r["clocks"] or {}
     sm_mhz = clk.get("sm_mhz") or 1965.0
-    roof, roof_other = summation_rooflines(r, sm_mhz, args)
+    roof, roof_other = rooflines(r, peaks, sm_mhz, args)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": r["workload"], "global_batch": world, "parallelism": f"replicas{world}",
+                   "nt": r["nt"], "ns": r["ns"], "beams": r["n_beams"],
                    "l2": "flushed (256 MiB write) between timed steps", "cutoff_efolds": args.cutoff},
         "e2e": {"value": world * r["dense_step"] / r["e2e_t"], "unit": UNIT, "h2d_bytes_per_step": r["h2d"],
                 "d2h_bytes_per_step": r["d2h"], "ms_per_step": r["e2e_t"] * 1e3},
@@ -502,9 +612,10 @@ def main():
         "roofline_other": roof_other,
         "kernels": {"fwd32_s": r["t_fwd_kernel"], "adj32_s": r["t_adj_kernel"], "fwd_evals": r["fwd_evals"],
                     "adj_evals": r["adj_evals"], "dense_evals_per_step": r["dense_step"],
-                    "fwd_evals_per_s": r["fwd_evals"] / r["t_fwd_kernel"],
-                    "adj_evals_per_s": r["adj_evals"] / r["t_adj_kernel"],
-                    "ode_s_per_step": r["t_ode"]},
+                    "fwd_evals_per_s": r["fwd_evals"] / r["t_fwd_kernel"] if r["t_fwd_kernel"] else None,
+                    "adj_evals_per_s": r["adj_evals"] / r["t_adj_kernel"] if r["t_adj_kernel"] else None,
+                    "ode_s_per_step": r["t_ode"], "ode_attempted_steps_per_step": r["ode_steps"]},
+        "peaks_measured": peaks,
         "clocks": clk,
         "cpu_baseline": cpu,
     }

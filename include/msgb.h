@@ -218,6 +218,8 @@ typedef struct msgb_ode_opts {
     int32_t dense_output;    /* DOPRI5 save times: 0 steps end on every save time (each
                                 step at most one save interval); 1 steps follow the error
                                 control and save times come from the continuous extension */
+    unsigned long long *step_count; /* optional device counter (NULL: none): attempted
+                                DOPRI5 steps (accepted + rejected) of the call are added to it */
 } msgb_ode_opts;
 
 /* FP64 integration of coupled_rhs_absorption (gb/gb_solvers.py:787-867) for
@@ -506,6 +508,22 @@ int msgb_tr_final_states(const msgb_problem *prob, const msgb_medium *med, const
 int msgb_scatter_coeff_grad(const int64_t *idx, const double *g, int64_t n, double scale,
                             const msgb_mswpt *plan, int apply_half_mask, double *G,
                             msgb_stream_t stream);
+
+/* ---- throughput probes (measurement; no counterpart in the reference) ---
+ * The roofline denominators of the FP32 summation, the FP64 beam ODE and the
+ * special-function unit, measured on the device that runs them: blocks x
+ * threads threads each run 8 independent chains of `iters` operations of one
+ * kind.  The caller times the launch on its stream and divides
+ * msgb_peak_probe_ops() (flops, FMA = 2; MUFU: operations) by the time.
+ * sink: (blocks * threads) floats, overwritten. */
+enum {
+    MSGB_PEAK_FP32 = 0,      /* scalar FFMA */
+    MSGB_PEAK_FP32X2 = 1,    /* paired FFMA2 (two FP32 lanes per instruction) */
+    MSGB_PEAK_FP64 = 2,      /* DFMA */
+    MSGB_PEAK_MUFU = 3       /* sin.approx (MUFU) */
+};
+double msgb_peak_probe_ops(int kind, int64_t iters, int blocks, int threads);
+int msgb_peak_probe(int kind, int64_t iters, int blocks, int threads, float *sink, msgb_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -242,21 +242,31 @@ def test_reference_propagator_names_are_accepted():
         assert s.closed_form is closed
 
 
-def test_bench_reports_the_dominant_summation_kernel():
-    """bench.py's roofline object is the summation kernel with the larger
-    device time, with its algorithmic flops per evaluated triple."""
+def test_bench_reports_the_dominant_kernel():
+    """bench.py's roofline object is the kernel with the largest device time
+    per step, with its algorithmic cost per work unit: the summation kernels
+    (flops per evaluated triple, measured FP32 peak) and, in heterogeneous
+    media, the beam ODE (flops per attempted step, measured FP64 peak)."""
     import types
 
     import bench
 
     args = types.SimpleNamespace(thr=65536, workload="c2")
-    r = {"hetero": False, "fwd_evals": 8e10, "adj_evals": 8e10, "t_fwd_kernel": 0.08, "t_adj_kernel": 0.09}
-    first, other = bench.summation_rooflines(r, 1965.0, args)
-    assert (first["kernel"], other["kernel"]) == ("adj32_kernel", "fwd32_kernel")
-    assert first["flops_per_eval"] == 40.0 and other["flops_per_eval"] == 36.0
-    assert abs(first["frac"] - 8e10 * 40 / 0.09 / 1e12 / (148 * 128 * 2 * 1965e6 / 1e12)) < 1e-12
+    peaks = {"fp32": 70.0, "fp32x2": 72.0, "fp32_best": 72.0, "fp64": 36.0, "mufu": 4.6, "method": "probe"}
+    r = {"hetero": False, "fwd_evals": 8e10, "adj_evals": 8e10, "t_fwd_kernel": 0.08, "t_adj_kernel": 0.09,
+         "t_ode": 0.0, "ode_steps": 0, "ndim": 2}
+    first, other = bench.rooflines(r, peaks, 1965.0, args)
+    assert (first["kernel"], other[0]["kernel"]) == ("adj32_kernel", "fwd32_kernel")
+    assert first["flops_per_eval"] == 40.0 and other[0]["flops_per_eval"] == 36.0
+    assert abs(first["frac"] - 8e10 * 40 / 0.09 / 1e12 / 72.0) < 1e-12
+    assert abs(first["mufu"]["frac"] - 3 * 8e10 / 0.09 / 1e12 / 4.6) < 1e-12
     r["t_fwd_kernel"] = 0.1
-    assert bench.summation_rooflines(r, 1965.0, args)[0]["kernel"] == "fwd32_kernel"
+    assert bench.rooflines(r, peaks, 1965.0, args)[0]["kernel"] == "fwd32_kernel"
+    r.update(hetero=True, t_ode=4.0, ode_steps=3e9)
+    first, other = bench.rooflines(r, peaks, 1965.0, args)
+    assert first["kernel"] == "dopri_kernel" and first["bound"] == "fp64"
+    assert abs(first["frac"] - 3e9 * bench.ode_flops_per_step(2) / 4.0 / 1e12 / 36.0) < 1e-12
+    assert [e["kernel"] for e in other] == ["fwd32_kernel<TRAJ>", "adj32_kernel<TRAJ>"]
 
 
 def test_infer_planar_surface_matches_reference():
