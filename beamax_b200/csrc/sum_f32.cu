@@ -775,214 +775,275 @@ fwd32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
 }
 
 // ------------------------------------------------------------------ adjoint
-// Tile-parallel transpose.  Persistent CTAs take (time tile, sensor tile)
-// items as the forward does; warp w owns sensor group w and lane l time l,
-// and holds d(t, s) for its GS sensors in registers for the whole item.  Each
-// pair of surviving beams runs the forward's recurrence while the lane
-// accumulates sum_s d(t, s) conj(z(t, s)); the pair's partials are reduced
-// over the 32 times (FP32 shuffles, fixed order), over the warps (FP64, fixed
-// order) and added to the beam's FP64 slot with one atomic per (beam, item).
-// g must be zeroed first; the order of those atomic additions varies between
-// runs (last-bit differences of the FP64 result).
+// Deterministic tile-parallel transpose (no floating-point atomics).
+//
+// Work item = (time tile tt, range of RJ consecutive beam indices j): for the
+// homogeneous entry point j is a selected coefficient and both of its modes
+// are summed; for trajectories j is a beam of the chunk.  Items run tt-major,
+// so consecutive items read the same time tile of the data.  For each sensor
+// tile in order, the CTA loads the tile's positions (shared memory) and data
+// (registers: warp w holds sensor group w, lane l time l), tests the range's
+// beams for survival, and for every pair of surviving beams runs the
+// forward's recurrence while the lane accumulates sum_s d(t, s) conj(z(t, s)).
+// The pair's partials are reduced over the 32 times (FP32 shuffles) and over
+// the 8 warps (FP64), in fixed orders, into the range's per-beam FP64
+// accumulators in shared memory (one owner thread per beam per pass).  The
+// item then writes every accumulator (zeros included) to part[tt][slot], and
+// reduce_parts_kernel sums part over the time tiles in order.  Each partial
+// has one writer and every sum has a fixed order, so the result is
+// bit-identical between runs; the work counter only hands out items.
+constexpr int NACC = 2048;  // accumulator slots (re, im FP64) per item
+
+template <bool TRAJ>
+struct AdjRange {
+    static constexpr int RJ = TRAJ ? NACC : NACC / 2;  // beam indices per item
+};
+
 template <int D, bool PERIODIC, bool TRAJ>
 __global__ void __launch_bounds__(THREADS, 2)
 adj32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *tiles, const int32_t *offs,
              const float *ds_g, const float *hn_g, const uint8_t *gfast_g, const float *dataT, float cutoff,
-             double *g, unsigned long long *eval_count, int *work, int n_st, int n_tiles, TrajSrc<D> T) {
+             double *part, unsigned long long *eval_count, int *work, int n_st, int n_ranges, int n_items,
+             TrajSrc<D> T) {
     constexpr int NF = Rec<D>::NF;
+    constexpr int RJ = AdjRange<TRAJ>::RJ;
     __shared__ float rec[NF][G][TT];
     __shared__ float sds[TS][D], shn[TS][D];
-    __shared__ int64_t surv[2 * THREADS];
+    __shared__ int32_t surv[2 * THREADS];
     __shared__ int warp_cnt[NW];
-    __shared__ double part[NW][G][2];
-    __shared__ int tile_s, nsurv_s;
+    __shared__ double wpart[NW][G][2];
+    __shared__ int item_s, nsurv_s;
+    extern __shared__ double acc_smem[];  // (NACC, 2)
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int64_t nbeam = TRAJ ? T.nb : B.n;
+    const int64_t nslots = TRAJ ? T.nb : 2 * B.n;
     unsigned long long evals = 0;
+    for (int q = tid; q < 2 * NACC; q += THREADS) acc_smem[q] = 0.0;
     while (true) {
-        if (tid == 0) tile_s = atomicAdd(work, 1);
+        if (tid == 0) item_s = atomicAdd(work, 1);
         __syncthreads();
-        const int tile = tile_s;
-        if (tile >= n_tiles) break;
-        const int64_t st = tile % n_st, tt = tile / n_st;
-        const int64_t s_first = offs[st], t_first = tt * TT;
-        const int s_cnt = offs[st + 1] - offs[st];
+        const int item = item_s;
+        if (item >= n_items) break;
+        const int64_t tt = item / n_ranges, r0 = (int64_t)(item % n_ranges) * RJ;
+        const int64_t r1 = min(r0 + RJ, nbeam);
+        const int64_t t_first = tt * TT;
         const int t_cnt = (int)min((int64_t)TT, P.nt - t_first);
-        const TileInfo<D> ti = tiles[st];
         const float ta = (float)P.ts[t_first], tb = (float)P.ts[t_first + t_cnt - 1];
-        for (int k = tid; k < TS; k += THREADS) {
-#pragma unroll
-            for (int i = 0; i < D; ++i) {
-                sds[k][i] = k < s_cnt ? ds_g[(s_first + k) * D + i] : 0.0f;
-                shn[k][i] = k < s_cnt ? hn_g[(s_first + k) * D + i] : 0.0f;
-            }
-        }
-        const bool fast = gfast_g[st * NW + warp] != 0;
-        const int gbase = warp * GS;
-        const bool active = gbase < s_cnt;
         const bool tv = lane < t_cnt;
-        const float *dcol = dataT + (int64_t)s_first * P.nt + t_first + lane;
-        float dv[GS];
+        for (int st = 0; st < n_st; ++st) {
+            const int64_t s_first = offs[st];
+            const int s_cnt = offs[st + 1] - offs[st];
+            if (s_cnt <= 0) continue;
+            const TileInfo<D> ti = tiles[st];
+            __syncthreads();  // the previous tile's passes are done with sds / shn
+            for (int k = tid; k < TS; k += THREADS) {
 #pragma unroll
-        for (int k = 0; k < GS; ++k)
-            dv[k] = (tv && gbase + k < s_cnt) ? __ldg(dcol + (int64_t)(gbase + k) * P.nt) : 0.0f;
-        const int64_t nbeam = TRAJ ? T.nb : B.n;
+                for (int i = 0; i < D; ++i) {
+                    sds[k][i] = k < s_cnt ? ds_g[(s_first + k) * D + i] : 0.0f;
+                    shn[k][i] = k < s_cnt ? hn_g[(s_first + k) * D + i] : 0.0f;
+                }
+            }
+            const bool fast = gfast_g[st * NW + warp] != 0;
+            const int gbase = warp * GS;
+            const bool active = gbase < s_cnt;
+            const float *dcol = dataT + (int64_t)s_first * P.nt + t_first + lane;
+            float dv[GS];
+#pragma unroll
+            for (int k = 0; k < GS; ++k)
+                dv[k] = (tv && gbase + k < s_cnt) ? __ldg(dcol + (int64_t)(gbase + k) * P.nt) : 0.0f;
 
-        for (int64_t j0 = 0; j0 < nbeam; j0 += THREADS) {
-            const int64_t j = j0 + tid;
-            bool keep_p = false, keep_m = false;
-            if (j < nbeam) {
-                if (TRAJ) {
-                    keep_p = traj_survives<D>(T, j, tt, ti, cutoff);
-                } else {
-                    const Cull<D> cb = cull[j];
-                    keep_p = mode_on(B.modes, 0) && survives<D>(cb, (float)P.c, ta, tb, ti, P, cutoff);
-                    keep_m = mode_on(B.modes, 1) && survives<D>(cb, -(float)P.c, ta, tb, ti, P, cutoff);
-                }
-            }
-            const unsigned bp = __ballot_sync(0xffffffffu, keep_p);
-            const unsigned bm = __ballot_sync(0xffffffffu, keep_m);
-            if (lane == 0) warp_cnt[warp] = __popc(bp) + __popc(bm);
-            __syncthreads();
-            int off = 0, tot = 0;
-#pragma unroll
-            for (int w = 0; w < NW; ++w) {
-                if (w < warp) off += warp_cnt[w];
-                tot += warp_cnt[w];
-            }
-            const unsigned lt = (1u << lane) - 1u;
-            if (keep_p) surv[off + __popc(bp & lt)] = j;
-            if (keep_m) surv[off + __popc(bp) + __popc(bm & lt)] = j + B.n;
-            if (tid == 0) nsurv_s = tot;
-            __syncthreads();
-            const int nsurv = nsurv_s;
-            evals += (unsigned long long)nsurv * (unsigned long long)t_cnt * (unsigned long long)s_cnt;
-            for (int g0 = 0; g0 < nsurv; g0 += G) {
-                {
-                    const int gl = tid / TT, tloc = tid % TT;
-                    Rec<D> r;
-                    if (g0 + gl < nsurv && tloc < t_cnt) {
-                        BeamTime<D> bt;
-                        if (TRAJ)
-                            traj_beam_time<D>(B, T, surv[g0 + gl], t_first + tloc, bt);
-                        else
-                            beam_time<D>(P, B, surv[g0 + gl], P.ts[t_first + tloc], bt);
-                        anchor<D>(P, bt, ti.s0, r);
+            for (int64_t j0 = r0; j0 < r1; j0 += THREADS) {
+                const int64_t j = j0 + tid;
+                bool keep_p = false, keep_m = false;
+                if (j < r1) {
+                    if (TRAJ) {
+                        keep_p = traj_survives<D>(T, j, tt, ti, cutoff);
                     } else {
-#pragma unroll
-                        for (int i = 0; i < D; ++i) r.d0[i] = 0.0f, r.wp[i] = 0.0f;
-#pragma unroll
-                        for (int q = 0; q < Sym<D>::S; ++q) r.q[q] = 0.0f, r.p[q] = 0.0f;
-                        r.th0 = 0.0f;
-                        r.amp = 0.0f;
+                        const Cull<D> cb = cull[j];
+                        keep_p = mode_on(B.modes, 0) && survives<D>(cb, (float)P.c, ta, tb, ti, P, cutoff);
+                        keep_m = mode_on(B.modes, 1) && survives<D>(cb, -(float)P.c, ta, tb, ti, P, cutoff);
                     }
-                    const float *rf = reinterpret_cast<const float *>(&r);
-#pragma unroll
-                    for (int f = 0; f < NF; ++f) rec[f][gl][tloc] = rf[f];
                 }
-                __syncthreads();
-                const int ng = min(G, nsurv - g0);
-                for (int gl = 0; gl < ng; gl += 2) {
-                    float2 ar = make_float2(0.0f, 0.0f), ai = make_float2(0.0f, 0.0f);
-                    if (active) {
-                        Rec<D> ra, rb;
-                        load_rec<D>(rec, gl, lane, ra);
-                        load_rec<D>(rec, gl + 1, lane, rb);  // zero-amplitude record when gl + 1 == ng
-                        cf za, fa, qa, zb, fb, qb;
-                        int ka = kRunRecurrence, kb = kRunRecurrence;
-                        if (fast) {
-                            za = seed_eval<D, false>(ra, sds[gbase], shn[gbase], true, P, fa, qa, &ka, cutoff > 0.0f);
-                            zb = seed_eval<D, false>(rb, sds[gbase], shn[gbase], true, P, fb, qb, &kb, cutoff > 0.0f);
-                            if (ka == kRunNegligible) za = fa = qa = cf{0.0f, 0.0f};
-                            if (kb == kRunNegligible) zb = fb = qb = cf{0.0f, 0.0f};
-                        }
-                        if (fast && ka != kRunDirect && kb != kRunDirect) {
-#if MSGB_F32X2
-                            cf2 z = pack2(za, zb), f = pack2(fa, fb);
-                            const cf2 q = pack2(qa, qb);
+                const unsigned bp = __ballot_sync(0xffffffffu, keep_p);
+                const unsigned bm = __ballot_sync(0xffffffffu, keep_m);
+                if (lane == 0) warp_cnt[warp] = __popc(bp) + __popc(bm);
+                __syncthreads();  // also: sds / shn loaded
+                int off = 0, tot = 0;
 #pragma unroll
-                            for (int k = 0; k < GS; ++k) {
-                                if (k > 0) {
-                                    z = cmul2(z, f);
-                                    f = cmul2(f, q);
-                                }
-                                const float2 dk = make_float2(dv[k], dv[k]);
-                                ar = __ffma2_rn(dk, z.re, ar);
-                                ai = __ffma2_rn(neg2(dk), z.im, ai);
+                for (int w = 0; w < NW; ++w) {
+                    if (w < warp) off += warp_cnt[w];
+                    tot += warp_cnt[w];
+                }
+                // local slot: beam j - r0 (mode +1 / trajectories), RJ + j - r0 (mode -1)
+                const unsigned lt = (1u << lane) - 1u;
+                if (keep_p) surv[off + __popc(bp & lt)] = (int32_t)(j - r0);
+                if (keep_m) surv[off + __popc(bp) + __popc(bm & lt)] = (int32_t)(RJ + j - r0);
+                if (tid == 0) nsurv_s = tot;
+                __syncthreads();
+                const int nsurv = nsurv_s;
+                evals += (unsigned long long)nsurv * (unsigned long long)t_cnt * (unsigned long long)s_cnt;
+                for (int g0 = 0; g0 < nsurv; g0 += G) {
+                    {
+                        const int gl = tid / TT, tloc = tid % TT;
+                        Rec<D> r;
+                        if (g0 + gl < nsurv && tloc < t_cnt) {
+                            const int q = surv[g0 + gl];
+                            const int64_t b = TRAJ ? r0 + q : (q < RJ ? r0 + q : B.n + r0 + q - RJ);
+                            BeamTime<D> bt;
+                            if (TRAJ)
+                                traj_beam_time<D>(B, T, b, t_first + tloc, bt);
+                            else
+                                beam_time<D>(P, B, b, P.ts[t_first + tloc], bt);
+                            anchor<D>(P, bt, ti.s0, r);
+                        } else {
+#pragma unroll
+                            for (int i = 0; i < D; ++i) r.d0[i] = 0.0f, r.wp[i] = 0.0f;
+#pragma unroll
+                            for (int q = 0; q < Sym<D>::S; ++q) r.q[q] = 0.0f, r.p[q] = 0.0f;
+                            r.th0 = 0.0f;
+                            r.amp = 0.0f;
+                        }
+                        const float *rf = reinterpret_cast<const float *>(&r);
+#pragma unroll
+                        for (int f = 0; f < NF; ++f) rec[f][gl][tloc] = rf[f];
+                    }
+                    __syncthreads();
+                    const int ng = min(G, nsurv - g0);
+                    for (int gl = 0; gl < ng; gl += 2) {
+                        float2 ar = make_float2(0.0f, 0.0f), ai = make_float2(0.0f, 0.0f);
+                        if (active) {
+                            Rec<D> ra, rb;
+                            load_rec<D>(rec, gl, lane, ra);
+                            load_rec<D>(rec, gl + 1, lane, rb);  // zero-amplitude record when gl + 1 == ng
+                            cf za, fa, qa, zb, fb, qb;
+                            int ka = kRunRecurrence, kb = kRunRecurrence;
+                            if (fast) {
+                                za = seed_eval<D, false>(ra, sds[gbase], shn[gbase], true, P, fa, qa, &ka, cutoff > 0.0f);
+                                zb = seed_eval<D, false>(rb, sds[gbase], shn[gbase], true, P, fb, qb, &kb, cutoff > 0.0f);
+                                if (ka == kRunNegligible) za = fa = qa = cf{0.0f, 0.0f};
+                                if (kb == kRunNegligible) zb = fb = qb = cf{0.0f, 0.0f};
                             }
+                            if (fast && ka != kRunDirect && kb != kRunDirect) {
+#if MSGB_F32X2
+                                cf2 z = pack2(za, zb), f = pack2(fa, fb);
+                                const cf2 q = pack2(qa, qb);
+#pragma unroll
+                                for (int k = 0; k < GS; ++k) {
+                                    if (k > 0) {
+                                        z = cmul2(z, f);
+                                        f = cmul2(f, q);
+                                    }
+                                    const float2 dk = make_float2(dv[k], dv[k]);
+                                    ar = __ffma2_rn(dk, z.re, ar);
+                                    ai = __ffma2_rn(neg2(dk), z.im, ai);
+                                }
 #else
 #pragma unroll
-                            for (int k = 0; k < GS; ++k) {
-                                if (k > 0) {
-                                    za = cmul(za, fa);
-                                    fa = cmul(fa, qa);
-                                    zb = cmul(zb, fb);
-                                    fb = cmul(fb, qb);
+                                for (int k = 0; k < GS; ++k) {
+                                    if (k > 0) {
+                                        za = cmul(za, fa);
+                                        fa = cmul(fa, qa);
+                                        zb = cmul(zb, fb);
+                                        fb = cmul(fb, qb);
+                                    }
+                                    ar.x = fmaf(dv[k], za.re, ar.x);
+                                    ai.x = fmaf(-dv[k], za.im, ai.x);
+                                    ar.y = fmaf(dv[k], zb.re, ar.y);
+                                    ai.y = fmaf(-dv[k], zb.im, ai.y);
                                 }
-                                ar.x = fmaf(dv[k], za.re, ar.x);
-                                ai.x = fmaf(-dv[k], za.im, ai.x);
-                                ar.y = fmaf(dv[k], zb.re, ar.y);
-                                ai.y = fmaf(-dv[k], zb.im, ai.y);
-                            }
 #endif
-                        } else {
-                            // rare: broken runs, out-of-range recurrences
-                            cf dummy_r, dummy_q;
+                            } else {
+                                // rare: broken runs, out-of-range recurrences
+                                cf dummy_r, dummy_q;
 #pragma unroll 1
-                            for (int k = 0; k < GS; ++k) {
-                                const int s = gbase + k;
-                                const float d = (tv && s < s_cnt) ? __ldg(dcol + (int64_t)s * P.nt) : 0.0f;
-                                const cf za = seed_eval<D, PERIODIC>(ra, sds[s], shn[s], false, P, dummy_r, dummy_q);
-                                const cf zb = seed_eval<D, PERIODIC>(rb, sds[s], shn[s], false, P, dummy_r, dummy_q);
-                                ar.x = fmaf(d, za.re, ar.x);
-                                ai.x = fmaf(-d, za.im, ai.x);
-                                ar.y = fmaf(d, zb.re, ar.y);
-                                ai.y = fmaf(-d, zb.im, ai.y);
+                                for (int k = 0; k < GS; ++k) {
+                                    const int s = gbase + k;
+                                    const float d = (tv && s < s_cnt) ? __ldg(dcol + (int64_t)s * P.nt) : 0.0f;
+                                    const cf za = seed_eval<D, PERIODIC>(ra, sds[s], shn[s], false, P, dummy_r, dummy_q);
+                                    const cf zb = seed_eval<D, PERIODIC>(rb, sds[s], shn[s], false, P, dummy_r, dummy_q);
+                                    ar.x = fmaf(d, za.re, ar.x);
+                                    ai.x = fmaf(-d, za.im, ai.x);
+                                    ar.y = fmaf(d, zb.re, ar.y);
+                                    ai.y = fmaf(-d, zb.im, ai.y);
+                                }
+                            }
+                        }
+                        // over the 32 times: paired FP32 adds (the partials are sums of
+                        // 16 terms; FP64 from here on)
+#pragma unroll
+                        for (int o = 16; o > 0; o >>= 1) {
+                            ar = __fadd2_rn(ar, make_float2(__shfl_xor_sync(0xffffffffu, ar.x, o),
+                                                            __shfl_xor_sync(0xffffffffu, ar.y, o)));
+                            ai = __fadd2_rn(ai, make_float2(__shfl_xor_sync(0xffffffffu, ai.x, o),
+                                                            __shfl_xor_sync(0xffffffffu, ai.y, o)));
+                        }
+                        if (lane == 0) {
+                            wpart[warp][gl][0] = (double)ar.x;
+                            wpart[warp][gl][1] = (double)ai.x;
+                            if (gl + 1 < G) {
+                                wpart[warp][gl + 1][0] = (double)ar.y;
+                                wpart[warp][gl + 1][1] = (double)ai.y;
                             }
                         }
                     }
-                    // over the 32 times: paired FP32 adds (the partials are sums of
-                    // 16 terms; FP64 from here on)
+                    __syncthreads();
+                    if (tid < ng) {
+                        double re = 0.0, im = 0.0;
 #pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) {
-                        ar = __fadd2_rn(ar, make_float2(__shfl_xor_sync(0xffffffffu, ar.x, o),
-                                                        __shfl_xor_sync(0xffffffffu, ar.y, o)));
-                        ai = __fadd2_rn(ai, make_float2(__shfl_xor_sync(0xffffffffu, ai.x, o),
-                                                        __shfl_xor_sync(0xffffffffu, ai.y, o)));
-                    }
-                    const double v[4] = {(double)ar.x, (double)ai.x, (double)ar.y, (double)ai.y};
-                    if (lane == 0) {
-                        part[warp][gl][0] = v[0];
-                        part[warp][gl][1] = v[1];
-                        if (gl + 1 < G) {
-                            part[warp][gl + 1][0] = v[2];
-                            part[warp][gl + 1][1] = v[3];
+                        for (int w = 0; w < NW; ++w) {
+                            re += wpart[w][tid][0];
+                            im += wpart[w][tid][1];
                         }
+                        const int q = surv[g0 + tid];  // distinct within a pass: one owner per slot
+                        acc_smem[2 * q] += re;
+                        acc_smem[2 * q + 1] += im;
                     }
-                }
-                __syncthreads();
-                if (tid < ng) {
-                    double re = 0.0, im = 0.0;
-#pragma unroll
-                    for (int w = 0; w < NW; ++w) {
-                        re += part[w][tid][0];
-                        im += part[w][tid][1];
-                    }
-                    const int64_t b = surv[g0 + tid];
-                    const int64_t slot = TRAJ ? b : (b < B.n ? b : b - B.n);
-                    if (re != 0.0) atomicAdd(g + 2 * slot, re);
-                    if (im != 0.0) atomicAdd(g + 2 * slot + 1, im);
                 }
             }
         }
         __syncthreads();
+        // every slot of the item, zeros included, then clear for the next item
+        for (int q = tid; q < NACC; q += THREADS) {
+            const int64_t jl = TRAJ ? q : (q < RJ ? q : q - RJ);
+            const int64_t j = r0 + jl;
+            if (j < r1) {
+                const int64_t slot = TRAJ ? j : (q < RJ ? j : B.n + j);
+                double *dst = part + 2 * (tt * nslots + slot);
+                dst[0] = acc_smem[2 * q];
+                dst[1] = acc_smem[2 * q + 1];
+            }
+            acc_smem[2 * q] = 0.0;
+            acc_smem[2 * q + 1] = 0.0;
+        }
     }
     if (eval_count && tid == 0 && evals) atomicAdd(eval_count, evals);
 }
 
+// g[j] = sum over time tiles, in order, of part[tt][j] (trajectories) or of
+// part[tt][j] + part[tt][n + j] (both modes of coefficient j).
+__global__ void reduce_parts_kernel(const double *part, int64_t n_tt, int64_t nslots, int64_t n_out, int both_modes,
+                                    double *g) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= n_out) return;
+    double re = 0.0, im = 0.0;
+    for (int64_t tt = 0; tt < n_tt; ++tt) {
+        const double *p = part + 2 * (tt * nslots + j);
+        re += p[0];
+        im += p[1];
+        if (both_modes) {
+            re += p[2 * n_out];
+            im += p[2 * n_out + 1];
+        }
+    }
+    g[2 * j] = re;
+    g[2 * j + 1] = im;
+}
+
 // ------------------------------------------------------------------ workspace
 struct Layout {
-    size_t keys_in, keys_out, vals_in, vals_out, cub, tiles, offs, gfast, ds, hn, seed, sorted, cull, data, work, total;
+    size_t keys_in, keys_out, vals_in, vals_out, cub, tiles, offs, gfast, ds, hn, seed, sorted, cull, data, work, part,
+        total;
     size_t cub_bytes;
     int64_t n_st;
 };
@@ -1019,8 +1080,15 @@ Layout layout(const msgb_problem *p, int64_t n_beams, bool with_data, int64_t n_
     l.cull = o; o = align256(o + (n_beams > 0 ? n_beams : 1) * sizeof(Cull<3>));
     l.data = o; o = align256(o + (with_data ? p->nt * ns * 4 : 0));
     l.work = o; o = align256(o + 64);
+    // adjoint partials: one complex FP64 per (time tile, beam mode) of the coefficients
+    l.part = o; o = align256(o + (with_data ? (size_t)((p->nt + TT - 1) / TT) * 2 * (n_beams > 0 ? n_beams : 0) * 16 : 0));
     l.total = o;
     return l;
+}
+
+// Adjoint partials of a trajectory chunk of nb beams: (n_tt, nb) complex FP64.
+size_t traj_part_bytes(const msgb_problem *p, int64_t nb) {
+    return align256((size_t)((p->nt + TT - 1) / TT) * (size_t)(nb > 0 ? nb : 0) * 16);
 }
 
 __global__ void copy_i32_kernel(const int32_t *in, int64_t n, int32_t *out) {
@@ -1124,7 +1192,7 @@ int run_fwd(const msgb_problem *p, const msgb_beam_set *b, const msgb_sum_opts *
 
 template <int D, bool TRAJ>
 int run_adj(const msgb_problem *p, const msgb_beam_set *b, const msgb_sum_opts *o, char *ws, const Layout &l,
-            const float *data, double *g, cudaStream_t st, TrajSrc<D> T) {
+            const float *data, double *part, double *g, cudaStream_t st, TrajSrc<D> T) {
     if (int e = prep<D>(p, b, o, l, ws, st)) return e;
     dim3 tg((unsigned)((p->ns + 31) / 32), (unsigned)((p->nt + 31) / 32));
     if (tg.y > 65535u) return fail(MSGB_ERR_UNSUPPORTED, "msgb_adj_gather_f32: nt too large");
@@ -1134,27 +1202,34 @@ int run_adj(const msgb_problem *p, const msgb_beam_set *b, const msgb_sum_opts *
     P.sensors = (const double *)(ws + l.sorted);
     bool periodic = false;
     for (int i = 0; i < D; ++i) periodic |= (p->periodic[i] != 0);
-    const int64_t nw = TRAJ ? T.nb : b->n;
+    const int64_t nw = TRAJ ? T.nb : b->n;  // beam indices j of the items
     const int64_t n_st = l.n_st, n_tt = (p->nt + TT - 1) / TT;
-    if (n_st * n_tt > 0x7fffffffLL) return fail(MSGB_ERR_UNSUPPORTED, "msgb_adj_gather_f32: too many tiles");
-    cudaMemsetAsync(g, 0, sizeof(double) * 2 * nw, st);
+    const int64_t n_ranges = (nw + AdjRange<TRAJ>::RJ - 1) / AdjRange<TRAJ>::RJ;
+    if (n_ranges * n_tt > 0x7fffffffLL || n_st > 0x7fffffffLL)
+        return fail(MSGB_ERR_UNSUPPORTED, "msgb_adj_gather_f32: too many work items");
     int *work = (int *)(ws + l.work);
     cudaMemsetAsync(work, 0, sizeof(int), st);
-    const int n_tiles = (int)(n_st * n_tt);
+    const int n_items = (int)(n_ranges * n_tt);
     const int64_t want = 2LL * sm_count();
-    const unsigned grid = (unsigned)(want < n_tiles ? want : n_tiles);
+    const unsigned grid = (unsigned)(want < n_items ? want : n_items);
+    const size_t smem = (size_t)NACC * 2 * sizeof(double);
     auto args = [&](auto kern) {
-        kern<<<grid, THREADS, 0, st>>>(P, to_args(b), (const Cull<D> *)(ws + l.cull), (const TileInfo<D> *)(ws + l.tiles),
-                                       (const int32_t *)(ws + l.offs), (const float *)(ws + l.ds),
-                                       (const float *)(ws + l.hn), (const uint8_t *)(ws + l.gfast),
-                                       (const float *)(ws + l.data), o ? (float)o->cutoff : 0.0f, g,
-                                       o ? o->eval_count : nullptr, work, (int)n_st, n_tiles, T);
+        kern<<<grid, THREADS, smem, st>>>(P, to_args(b), (const Cull<D> *)(ws + l.cull),
+                                          (const TileInfo<D> *)(ws + l.tiles), (const int32_t *)(ws + l.offs),
+                                          (const float *)(ws + l.ds), (const float *)(ws + l.hn),
+                                          (const uint8_t *)(ws + l.gfast), (const float *)(ws + l.data),
+                                          o ? (float)o->cutoff : 0.0f, part, o ? o->eval_count : nullptr, work,
+                                          (int)n_st, (int)n_ranges, n_items, T);
     };
     if (periodic)
         args(adj32_kernel<D, true, TRAJ>);
     else
         args(adj32_kernel<D, false, TRAJ>);
-    return check_launch("msgb_adj_gather_f32");
+    if (int e = check_launch("msgb_adj_gather_f32")) return e;
+    const int blk = 256;
+    reduce_parts_kernel<<<(unsigned)((nw + blk - 1) / blk), blk, 0, st>>>(part, n_tt, TRAJ ? nw : 2 * nw, nw,
+                                                                          TRAJ ? 0 : 1, g);
+    return check_launch("msgb_adj_gather_f32 reduce");
 }
 
 template <int D>
@@ -1230,30 +1305,36 @@ extern "C" int msgb_adj_gather_f32(const msgb_problem *prob, const msgb_beam_set
     cudaStream_t st = as_stream(stream);
     char *ws = (char *)workspace;
     switch (prob->ndim) {
-        case 1: return run_adj<1, false>(prob, beams, opts, ws, l, data, g, st, traj_src<1>(nullptr, nullptr, 1, 1));
-        case 2: return run_adj<2, false>(prob, beams, opts, ws, l, data, g, st, traj_src<2>(nullptr, nullptr, 1, 1));
-        default: return run_adj<3, false>(prob, beams, opts, ws, l, data, g, st, traj_src<3>(nullptr, nullptr, 1, 1));
+        case 1: return run_adj<1, false>(prob, beams, opts, ws, l, data, (double *)(ws + l.part), g, st,
+                                         traj_src<1>(nullptr, nullptr, 1, 1));
+        case 2: return run_adj<2, false>(prob, beams, opts, ws, l, data, (double *)(ws + l.part), g, st,
+                                         traj_src<2>(nullptr, nullptr, 1, 1));
+        default: return run_adj<3, false>(prob, beams, opts, ws, l, data, (double *)(ws + l.part), g, st,
+                                          traj_src<3>(nullptr, nullptr, 1, 1));
     }
 }
 
 // ---- trajectory entry points ------------------------------------------------
 static size_t traj_state_offset(const Layout &l) { return l.total; }
 
+static size_t traj_state_bytes(const msgb_problem *p) { return align256((size_t)2 * p->nt * p->ns * sizeof(float)); }
+
 extern "C" size_t msgb_sum_f32_traj_workspace_size(const msgb_problem *prob, int64_t nb_max) {
     if (validate_problem(prob) || nb_max < 0) return 0;
     const Layout l = layout(prob, 0, true, (prob->ns + GS - 1) / GS);
-    return l.total + align256((size_t)2 * prob->nt * prob->ns * sizeof(float));
+    return l.total + traj_state_bytes(prob) + traj_part_bytes(prob, nb_max);
 }
 
+// with_part: the adjoint's partials (n_tt, nb) follow the Kahan state.
 static int check_traj32(const msgb_problem *p, const msgb_beam_set *b, const msgb_trajectories *t,
-                        const msgb_sum_opts *o, void *ws, size_t bytes, Layout &l) {
+                        const msgb_sum_opts *o, void *ws, size_t bytes, bool with_part, Layout &l) {
     if (!t || !t->rec32) return fail(MSGB_ERR_ARG, "FP32 trajectory records are NULL");
     if (!t->cull && o && o->cutoff > 0.0) return fail(MSGB_ERR_ARG, "culling boxes are NULL");
     if (t->nb < 0 || t->b_first < 0 || t->b_first + t->nb > 2 * b->n)
         return fail(MSGB_ERR_ARG, "trajectory beam range outside [0, 2n)");
     l = layout(p, 0, true, tile_count(p, o));
     if (l.n_st <= 0) return fail(MSGB_ERR_ARG, "sensor tiling has no tiles");
-    const size_t need = l.total + align256((size_t)2 * p->nt * p->ns * sizeof(float));
+    const size_t need = l.total + traj_state_bytes(p) + (with_part ? traj_part_bytes(p, t->nb) : 0);
     if (!ws || bytes < need) return fail(MSGB_ERR_WORKSPACE, "workspace too small: need %zu bytes, got %zu", need, bytes);
     if (((uintptr_t)ws & 255) != 0) return fail(MSGB_ERR_WORKSPACE, "workspace must be 256-byte aligned");
     return MSGB_OK;
@@ -1268,7 +1349,7 @@ extern "C" int msgb_sum_fwd_f32_traj(const msgb_problem *prob, const msgb_beam_s
     if (!out) return fail(MSGB_ERR_ARG, "msgb_sum_fwd_f32_traj: out is NULL");
     if (prob->nt == 0 || prob->ns == 0) return MSGB_OK;
     Layout l;
-    if (int e = check_traj32(prob, beams, traj, opts, workspace, workspace_bytes, l)) return e;
+    if (int e = check_traj32(prob, beams, traj, opts, workspace, workspace_bytes, false, l)) return e;
     cudaStream_t st = as_stream(stream);
     char *ws = (char *)workspace;
     float *state = (float *)(ws + traj_state_offset(l));
@@ -1292,13 +1373,14 @@ extern "C" int msgb_adj_gather_f32_traj(const msgb_problem *prob, const msgb_bea
         return check_launch("msgb_adj_gather_f32_traj");
     }
     Layout l;
-    if (int e = check_traj32(prob, beams, traj, opts, workspace, workspace_bytes, l)) return e;
+    if (int e = check_traj32(prob, beams, traj, opts, workspace, workspace_bytes, true, l)) return e;
     cudaStream_t st = as_stream(stream);
     char *ws = (char *)workspace;
+    double *part = (double *)(ws + traj_state_offset(l) + traj_state_bytes(prob));
     switch (prob->ndim) {
-        case 1: return run_adj<1, true>(prob, beams, opts, ws, l, data, g, st, traj_src<1>(traj, nullptr, 1, 1));
-        case 2: return run_adj<2, true>(prob, beams, opts, ws, l, data, g, st, traj_src<2>(traj, nullptr, 1, 1));
-        default: return run_adj<3, true>(prob, beams, opts, ws, l, data, g, st, traj_src<3>(traj, nullptr, 1, 1));
+        case 1: return run_adj<1, true>(prob, beams, opts, ws, l, data, part, g, st, traj_src<1>(traj, nullptr, 1, 1));
+        case 2: return run_adj<2, true>(prob, beams, opts, ws, l, data, part, g, st, traj_src<2>(traj, nullptr, 1, 1));
+        default: return run_adj<3, true>(prob, beams, opts, ws, l, data, part, g, st, traj_src<3>(traj, nullptr, 1, 1));
     }
 }
 

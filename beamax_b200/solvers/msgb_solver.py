@@ -540,7 +540,7 @@ class MSGBSolver:
         tiling = self._tiling(domain, sensors, dev)
         opts = _lib.SumOpts(cutoff=self.cutoff, eval_count=cnt.data_ptr(),
                             tiling=_lib.ref(tiling[0]) if tiling else None)
-        nbytes = _lib.lib().msgb_sum_f32_traj_workspace_size(_lib.ref(pr), 2 * bt.n)
+        nbytes = _lib.lib().msgb_sum_f32_traj_workspace_size(_lib.ref(pr), max(nb for _, nb in chunks))
         ws = workspace(dev, "sum32traj", nbytes)
         for i, (b_first, nb) in enumerate(chunks):
             tr, buf = self._trajectories(pr, med, bs, b_first, nb, False, per, n_tt, dev, st, status,
@@ -607,7 +607,7 @@ class MSGBSolver:
         tiling = None if fp64 else self._tiling(domain, sensors, dev)
         opts = _lib.SumOpts(cutoff=self.cutoff, eval_count=cnt.data_ptr(),
                             tiling=_lib.ref(tiling[0]) if tiling else None)
-        nbytes = 0 if fp64 else _lib.lib().msgb_sum_f32_traj_workspace_size(_lib.ref(pr), 2 * n)
+        nbytes = 0 if fp64 else _lib.lib().msgb_sum_f32_traj_workspace_size(_lib.ref(pr), max(nb for _, nb in chunks))
         ws = None if fp64 else workspace(dev, "sum32traj", nbytes)
         status = torch.zeros(2 * n, dtype=torch.int32, device=dev)
         self._begin_trajectories(domain, ts)

@@ -144,10 +144,14 @@ int msgb_sum_fwd_f32(const msgb_problem *prob, const msgb_beam_set *beams,
 int msgb_sum_fwd_f32_static(const msgb_problem *prob, const msgb_beam_set *beams,
                             const msgb_sum_opts *opts, float *out, msgb_stream_t stream);
 
-/* FP32 transpose of msgb_sum_fwd_f32 (same culling), tile-parallel like the
- * forward: per-beam partials are added to g with FP64 atomics, so results
- * agree between runs to the last bits of FP64, not bit for bit.  data:
- * (nt, ns) FP32.  g: (n) complex FP64, written by the call (zeroed first). */
+/* FP32 transpose of msgb_sum_fwd_f32 (same culling), a deterministic
+ * per-beam gather: work items are (time tile, range of beams); each item
+ * sums its beams' conj(kernel) x data over every sensor tile and time of its
+ * tile in a fixed order into one partial per (time tile, beam mode), and a
+ * second kernel adds the partials over the time tiles in order.  No
+ * floating-point atomics: results are bit-identical between runs.  data:
+ * (nt, ns) FP32.  g: (n) complex FP64, overwritten.  The workspace holds the
+ * partials (16 B per time tile of 32 samples and beam mode). */
 int msgb_adj_gather_f32(const msgb_problem *prob, const msgb_beam_set *beams,
                         const msgb_sum_opts *opts, void *workspace, size_t workspace_bytes,
                         const float *data, double *g, msgb_stream_t stream);
@@ -252,7 +256,9 @@ int msgb_sum_fwd_f32_traj(const msgb_problem *prob, const msgb_beam_set *beams,
                           int last_chunk, void *workspace, size_t workspace_bytes, float *out,
                           msgb_stream_t stream);
 /* g[b - b_first] for the chunk's beams (complex FP64, one entry per beam, not
- * per coefficient: the caller adds the two modes). */
+ * per coefficient: the caller adds the two modes), deterministic as
+ * msgb_adj_gather_f32; the workspace (sized for nb_max beams per chunk) holds
+ * the partials. */
 int msgb_adj_gather_f32_traj(const msgb_problem *prob, const msgb_beam_set *beams,
                              const msgb_trajectories *traj, const msgb_sum_opts *opts,
                              void *workspace, size_t workspace_bytes, const float *data, double *g,
