@@ -282,12 +282,12 @@ __host__ __device__ constexpr double sym_weight(int e) {
          : 1.0);
 }
 
-// Magnitude of complex entry e of the state (x and p entries are real).
+// Squared magnitude of complex entry e of the state (x and p entries are real).
 template <int D>
-__device__ __forceinline__ double entry_abs(const double *v, int e) {
-    if (e < 2 * D) return fabs(v[e]);
+__device__ __forceinline__ double entry_abs2(const double *v, int e) {
+    if (e < 2 * D) return v[e] * v[e];
     const int q = 2 * D + 2 * (e - 2 * D);
-    return hypot(v[q], v[q + 1]);
+    return fma(v[q], v[q], v[q + 1] * v[q + 1]);
 }
 
 // Continuous-extension weights (Shampine 1986, the dense output of Hairer,
@@ -316,7 +316,7 @@ constexpr size_t dopri_smem_bytes(int blk) {
 
 template <int D, int KIND>
 struct DopriBeam {
-    SState<D> y, f0;
+    SState<D> y;   // f(y) (first same as last) is stage 0 in shared memory
     double t, h, mode;
     int64_t steps, k;
     bool rejected;
@@ -332,7 +332,11 @@ struct DopriBeam {
         k = 1;
         rejected = false;
         code = 0;
+        SState<D> f0;
         rhs_sym<D, KIND>(med, mode, y, f0);
+        const double *fv = vals(f0);
+#pragma unroll
+        for (int c = 0; c < NVS<D>::value; ++c) ks[c * kst] = fv[c];
     }
 
     // One attempt; returns true when the beam is finished (all save times
@@ -364,11 +368,6 @@ struct DopriBeam {
         // limited the kernel to 8 warps per SM).
         SState<D> yt;
         const double *yv = vals(y);
-        {
-            const double *fv = vals(f0);
-#pragma unroll
-            for (int c = 0; c < N; ++c) ks[c * kst] = fv[c];
-        }
 #pragma unroll 1
         for (int s = 1; s < 7; ++s) {
             double acc[N];
@@ -403,11 +402,12 @@ struct DopriBeam {
                 for (int j = 0; j < 7; ++j) acc += DP_E[j] * KSV(j, c);
                 ev[c] = hh * acc;
             }
+            // (|e| / (atol + rtol max(|y0|, |y1|)))^2 from squared magnitudes:
+            // one square root per entry instead of three
 #pragma unroll
             for (int e = 0; e < NE; ++e) {
-                const double sc = o.atol + o.rtol * fmax(entry_abs<D>(yv, e), entry_abs<D>(nv, e));
-                const double r = entry_abs<D>(ev, e) / sc;
-                sum += sym_weight<D>(e) * (r * r);
+                const double sc = o.atol + o.rtol * sqrt(fmax(entry_abs2<D>(yv, e), entry_abs2<D>(nv, e)));
+                sum += sym_weight<D>(e) * (entry_abs2<D>(ev, e) / (sc * sc));
             }
         }
         const double err = sqrt(sum / NE_FULL);
@@ -452,11 +452,8 @@ struct DopriBeam {
             }
             t = t_new;
             y = yt;
-            {
-                double *fv = vals(f0);
 #pragma unroll
-                for (int c = 0; c < N; ++c) fv[c] = KSV(6, c);
-            }
+            for (int c = 0; c < N; ++c) KSV(0, c) = KSV(6, c);  // first same as last
 #undef KSV
             h = (last && !o.dense_output) ? fmax(hh * fac, h) : hh * fac;
         } else {

@@ -54,11 +54,13 @@ __device__ __forceinline__ void speed_eval_k(const MediumArgs &m, const double *
         const double t = u - fl;
         const int i0 = (int)fl;
         if (cubic) {
+            // 6 x the B-spline weights (the factors 1/6 are applied to the
+            // sums at the end: no FP64 division per weight)
             const double omt = 1.0 - t, t2 = t * t, t3 = t2 * t;
-            w[a][0] = omt * omt * omt / 6.0;
-            w[a][1] = (3.0 * t3 - 6.0 * t2 + 4.0) / 6.0;
-            w[a][2] = (-3.0 * t3 + 3.0 * t2 + 3.0 * t + 1.0) / 6.0;
-            w[a][3] = t3 / 6.0;
+            w[a][0] = omt * omt * omt;
+            w[a][1] = 3.0 * t3 - 6.0 * t2 + 4.0;
+            w[a][2] = -3.0 * t3 + 3.0 * t2 + 3.0 * t + 1.0;
+            w[a][3] = t3;
             d1[a][0] = -(omt * omt) / 2.0;
             d1[a][1] = 1.5 * t2 - 2.0 * t;
             d1[a][2] = -1.5 * t2 + t + 0.5;
@@ -151,14 +153,21 @@ __device__ __forceinline__ void speed_eval_k(const MediumArgs &m, const double *
             hh[Z][Z] = fma(w[0][i], tzz, hh[Z][Z]);
         }
     }
-    c = cc;
+    // Cubic weights were 6 x the true ones: a sum whose terms carry the plain
+    // weight of q axes is 6^q too large (value: D axes; gradient: D - 1;
+    // diagonal Hessian: D - 1; mixed Hessian: D - 2).
+    constexpr double s6 = cubic ? 1.0 / 6.0 : 1.0;
+    constexpr double sv = D == 1 ? s6 : (D == 2 ? s6 * s6 : s6 * s6 * s6);
+    constexpr double sg = D == 1 ? 1.0 : (D == 2 ? s6 : s6 * s6);
+    constexpr double sm = D == 3 ? s6 : 1.0;
+    c = cc * sv;
 #pragma unroll
     for (int a = 0; a < D; ++a) {
-        g[a] = gg[a] * m.inv_spacing[a];
+        g[a] = gg[a] * (sg * m.inv_spacing[a]);
 #pragma unroll
         for (int b = 0; b < D; ++b) {
             const double hv = a <= b ? hh[a][b] : hh[b][a];
-            H[a * D + b] = hv * (m.inv_spacing[a] * m.inv_spacing[b]);
+            H[a * D + b] = hv * ((a == b ? sg : sm) * m.inv_spacing[a] * m.inv_spacing[b]);
         }
     }
 }
@@ -287,8 +296,11 @@ struct RecordWriter {
                     f[q] = (float)(fac * mre);
                     f[S + q] = (float)(fac * mim);
                 }
-            f[2 * S] = (float)atan2(y.A.im, (y.A.re == 0.0 && y.A.im == 0.0) ? 1e-12 : y.A.re);
-            f[2 * S + 1] = (float)(2.0 * hypot(y.A.re, y.A.im));
+            // arg A and 2|A| are stored as floats: FP32 arithmetic on the
+            // rounded components gives them to FP32 precision
+            const float are = (float)y.A.re, aim = (float)y.A.im;
+            f[2 * S] = atan2f(aim, (are == 0.0f && aim == 0.0f) ? 1e-12f : are);
+            f[2 * S + 1] = 2.0f * hypotf(are, aim);
         }
         if (T.cull) {
             double Sm[D][D];
