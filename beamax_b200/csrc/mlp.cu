@@ -12,7 +12,11 @@
 // thread issues tcgen05.mma (M = 128, N <= 256, K = 16 per instruction) and
 // commits to an mbarrier; the others wait on it with a bounded spin.  Warp w
 // reads TMEM lanes 32w..32w+31 (its rows) with tcgen05.ld.
+#include <cuda.h>
 #include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
 
 #include "common.cuh"
 
@@ -164,6 +168,291 @@ __global__ void __launch_bounds__(GT) gemm_tc_kernel(GemmArgs g) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// TMA-fed persistent GEMM for K-contiguous operands with K <= 256 (every layer
+// of the surrogate's forward pass): C = A B^T (+ bias, act).
+//
+// Warp roles (192 threads, one CTA per SM):
+//   warp 0   - one lane issues the TMA loads: B (N x K, the layer's weights)
+//              once into shared memory, where it stays for every tile; A in
+//              128 x 64 chunks through a 4-stage ring (full / empty mbarriers);
+//   warp 1   - one lane issues tcgen05.mma (M = 128, N, K = 16 per
+//              instruction) into one of two TMEM accumulators (2 x 256
+//              columns) and commits each stage back to the ring;
+//   warps 2-5 - the epilogue: tcgen05.ld of their 32 TMEM lanes, bias, SiLU,
+//              FP32 / BF16 stores, then release the accumulator, so the MMAs
+//              of the next tile overlap this tile's epilogue.
+// Operands use the 128-byte swizzle (TMA box rows of 64 BF16 = 128 B); the
+// UMMA descriptors address 8-row atoms of 1024 B (SBO) and advance 32 B per
+// K = 16 step inside the swizzled row.  Every mbarrier wait is bounded: on
+// timeout the kernel raises the error flag, lets its issued copies land,
+// frees TMEM and returns.
+constexpr int TG_BM = 128;
+constexpr int TG_BK = 64;
+constexpr int TG_STAGES = 4;
+constexpr int TG_MAXKB = 4;  // K <= 256
+constexpr int TG_THREADS = 192;
+constexpr uint32_t TG_A_STAGE = TG_BM * TG_BK * 2;  // 16 KB
+constexpr size_t TG_SMEM = (size_t)TG_STAGES * TG_A_STAGE + (size_t)TG_MAXKB * 256 * TG_BK * 2 + 256 + 1024;
+
+struct TmaGemmArgs {
+    int M, N, K, kb, n_tiles;
+    const float *bias;
+    int act;
+    float *C32;
+    int64_t ldc32;
+    __nv_bfloat16 *C16;
+    int64_t ldc16;
+    int *err;
+};
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// Bounded wait for the phase of the given parity; false on timeout or when
+// another role has aborted.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort) {
+    for (int it = 0; it < (1 << 22); ++it) {
+        if (mbar_try(bar, parity)) return true;
+        if ((it & 63) == 63) {
+            if (*abort) return false;
+            __nanosleep(64);
+        }
+    }
+    return false;
+}
+
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1 << 16;                 // LBO (unused with the 128-byte swizzle)
+    d |= (uint64_t)(1024u >> 4) << 32;      // SBO: next 8-row atom
+    d |= (uint64_t)1 << 46;                 // descriptor version for sm_100
+    d |= (uint64_t)2 << 61;                 // 128-byte swizzle
+    return d;
+}
+
+__global__ void __launch_bounds__(TG_THREADS, 1)
+gemm_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, TmaGemmArgs g) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t *sA = smem;
+    uint8_t *sB = smem + TG_STAGES * TG_A_STAGE;
+    uint64_t *bars = (uint64_t *)(sB + TG_MAXKB * 256 * TG_BK * 2);
+    // bars: full[4], empty[4], bfull, tfull[2], tempty[2], mma_done
+    uint32_t *tslot = (uint32_t *)(bars + 14);
+    volatile int *abort = (volatile int *)(tslot + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t b_full = smem_u32(bars + 8);
+    auto full = [&](int s) { return smem_u32(bars + s); };
+    auto empty = [&](int s) { return smem_u32(bars + 4 + s); };
+    auto tfull = [&](int a) { return smem_u32(bars + 9 + a); };
+    auto tempty = [&](int a) { return smem_u32(bars + 11 + a); };
+    const uint32_t mma_done = smem_u32(bars + 13);
+    const uint32_t bbytes = (uint32_t)g.N * TG_BK * 2;
+
+    if (tid == 0) {
+        for (int s = 0; s < TG_STAGES; ++s) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(full(s)));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(empty(s)));
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b_full));
+        for (int a = 0; a < 2; ++a) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tfull(a)));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(tempty(a)));
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mma_done));
+        *abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;");
+        asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&tmA) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&tmB) : "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(tslot)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = *tslot;
+    const int n_local = g.n_tiles > (int)blockIdx.x ? (g.n_tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            bool ok = true;
+            // weights once
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b_full),
+                         "r"(bbytes * g.kb) : "memory");
+            for (int c = 0; c < g.kb; ++c)
+                asm volatile(
+                    "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+                    "[%4];" ::"r"(smem_u32(sB + (size_t)c * bbytes)),
+                    "l"((uint64_t)&tmB), "r"(c * TG_BK), "r"(0), "r"(b_full)
+                    : "memory");
+            int q = 0;
+            for (int it = 0; it < n_local && ok; ++it) {
+                const int m0 = ((int)blockIdx.x + it * (int)gridDim.x) * TG_BM;
+                for (int c = 0; c < g.kb; ++c, ++q) {
+                    const int s = q % TG_STAGES, round = q / TG_STAGES;
+                    if (!mbar_wait(empty(s), (round & 1) ^ 1, abort)) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(full(s)),
+                                 "r"(TG_A_STAGE) : "memory");
+                    asm volatile(
+                        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+                        "%3}], [%4];" ::"r"(smem_u32(sA + (size_t)s * TG_A_STAGE)),
+                        "l"((uint64_t)&tmA), "r"(c * TG_BK), "r"(m0), "r"(full(s))
+                        : "memory");
+                }
+            }
+            if (!ok) {
+                *abort = 1;
+                if (g.err) atomicOr(g.err, 1);
+            }
+            // every issued load lands before the CTA can exit
+            volatile int never = 0;
+            mbar_wait(b_full, 0, &never);
+            for (int k = q - TG_STAGES; k < q; ++k)
+                if (k >= 0) mbar_wait(full(k % TG_STAGES), (k / TG_STAGES) & 1, &never);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            bool ok = mbar_wait(b_full, 0, abort);
+            const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(g.N >> 3) << 17) |
+                                   ((uint32_t)(TG_BM >> 4) << 24);
+            int q = 0;
+            for (int it = 0; it < n_local && ok; ++it) {
+                const int a = it & 1, use = it >> 1;
+                if (!mbar_wait(tempty(a), (use & 1) ^ 1, abort)) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;");
+                const uint32_t dtm = tmem + (uint32_t)(a * 256);
+                for (int c = 0; c < g.kb; ++c, ++q) {
+                    const int s = q % TG_STAGES, round = q / TG_STAGES;
+                    if (!mbar_wait(full(s), round & 1, abort)) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;");
+                    const uint32_t abase = smem_u32(sA + (size_t)s * TG_A_STAGE);
+                    const uint32_t bbase = smem_u32(sB + (size_t)c * bbytes);
+#pragma unroll
+                    for (int kk = 0; kk < TG_BK / 16; ++kk) {
+                        const uint64_t da = sw128_desc(abase + 32u * kk);
+                        const uint64_t db = sw128_desc(bbase + 32u * kk);
+                        const uint32_t accum = (c > 0 || kk > 0) ? 1u : 0u;
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dtm),
+                            "l"(da), "l"(db), "r"(idesc), "r"(accum));
+                    }
+                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                        empty(s)) : "memory");
+                }
+                if (!ok) break;
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                    tfull(a)) : "memory");
+            }
+            if (!ok) {
+                *abort = 1;
+                if (g.err) atomicOr(g.err, 1);
+            }
+            // every issued MMA has finished before TMEM is released
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                mma_done) : "memory");
+            volatile int never = 0;
+            mbar_wait(mma_done, 0, &never);
+        }
+    } else {
+        const int quarter = warp & 3;  // TMEM lanes 32 quarter .. + 31
+        bool ok = true;
+        for (int it = 0; it < n_local && ok; ++it) {
+            const int a = it & 1, use = it >> 1;
+            const int m0 = ((int)blockIdx.x + it * (int)gridDim.x) * TG_BM;
+            ok = mbar_wait(tfull(a), use & 1, abort);
+            __syncwarp();
+            ok = __all_sync(0xffffffffu, ok);
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const int row = m0 + 32 * quarter + lane;
+            for (int col0 = 0; col0 < g.N; col0 += 16) {
+                uint32_t r[16];
+                const uint32_t taddr = tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(a * 256 + col0);
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                    "[%16];"
+                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                      "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                      "=r"(r[15])
+                    : "r"(taddr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;");
+                if (row < g.M) {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        const int col = col0 + j;
+                        float z = __uint_as_float(r[j]) + (g.bias ? g.bias[col] : 0.0f);
+                        if (g.C32) g.C32[row * g.ldc32 + col] = z;
+                        if (g.C16) g.C16[row * g.ldc16 + col] = __float2bfloat16(g.act == 1 ? silu(z) : z);
+                    }
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;");
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tempty(a)) : "memory");
+        }
+        if (!ok && lane == 0) {
+            *abort = 1;
+            if (g.err) atomicOr(g.err, 1);
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem));
+    }
+}
+
+// Host: cuTensorMapEncodeTiled from the driver, looked up once.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static std::once_flag once;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    });
+    return fn;
+}
+
+// Row-major BF16 matrix (rows x K, row stride ld elements) as a 2D tensor map
+// with boxes of `box_rows` x 64 and the 128-byte swizzle.
+bool bf16_tensor_map(CUtensorMap *map, const void *base, int64_t rows, int64_t K, int64_t ld, int box_rows) {
+    auto enc = tensor_map_encoder();
+    if (!enc) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+    cuuint32_t box[2] = {(cuuint32_t)TG_BK, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // dZ = dA * silu'(Z) (FP32 in, BF16 and FP32 out).
 __global__ void silu_backward_kernel(const float *dA, const float *Z, int64_t n, float *dZ32, __nv_bfloat16 *dZ16) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -231,6 +520,40 @@ extern "C" int msgb_gemm_bf16(const msgb_gemm *p, msgb_stream_t stream) {
     g.C16 = (__nv_bfloat16 *)p->C16;
     g.ldc16 = p->ldc16;
     g.err = p->error_flag;
+    // K-contiguous operands with 16-byte aligned rows and K <= 256: the TMA-fed
+    // persistent kernel; other layouts (the weight-gradient products) stage
+    // element by element.
+    const bool tma = p->sAk == 1 && p->sBk == 1 && p->K <= TG_MAXKB * TG_BK && p->sAm >= p->K && p->sBn >= p->K &&
+                     (p->sAm % 8) == 0 && (p->sBn % 8) == 0 && ((uintptr_t)p->A % 16) == 0 &&
+                     ((uintptr_t)p->B % 16) == 0 && p->M < (1 << 30);
+    if (tma) {
+        CUtensorMap ta, tb;
+        if (bf16_tensor_map(&ta, p->A, p->M, p->K, p->sAm, TG_BM) &&
+            bf16_tensor_map(&tb, p->B, p->N, p->K, p->sBn, p->N)) {
+            TmaGemmArgs t{};
+            t.M = p->M;
+            t.N = p->N;
+            t.K = p->K;
+            t.kb = (p->K + TG_BK - 1) / TG_BK;
+            t.n_tiles = (p->M + TG_BM - 1) / TG_BM;
+            t.bias = p->bias;
+            t.act = p->act;
+            t.C32 = p->C32;
+            t.ldc32 = p->ldc32;
+            t.C16 = (__nv_bfloat16 *)p->C16;
+            t.ldc16 = p->ldc16;
+            t.err = p->error_flag;
+            cudaError_t e = cudaFuncSetAttribute(gemm_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)TG_SMEM);
+            if (e != cudaSuccess) return fail(MSGB_ERR_CUDA, "msgb_gemm_bf16: %s", cudaGetErrorString(e));
+            int dev = 0, sms = 148;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            const unsigned grid = (unsigned)(t.n_tiles < sms ? t.n_tiles : sms);
+            gemm_tma_kernel<<<grid, TG_THREADS, TG_SMEM, as_stream(stream)>>>(ta, tb, t);
+            return check_launch("msgb_gemm_bf16");
+        }
+    }
     const size_t smem = sizeof(__nv_bfloat16) * (GM + 256) * KC + 16;
     cudaError_t e = cudaFuncSetAttribute(gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return fail(MSGB_ERR_CUDA, "msgb_gemm_bf16: %s", cudaGetErrorString(e));

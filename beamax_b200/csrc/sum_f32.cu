@@ -1435,6 +1435,18 @@ extern "C" int msgb_sum_fwd_f32_static(const msgb_problem *prob, const msgb_beam
                     "msgb_sum_fwd_f32_static: %lld coefficients and %lld sensors need %zu bytes of scratch, more "
                     "than the %zu-byte static scratch; call msgb_sum_fwd_f32 with a workspace instead",
                     (long long)beams->n, (long long)prob->ns, need.total, (size_t)MSGB_SUM_F32_STATIC_SCRATCH_BYTES);
+    cudaStream_t st = as_stream(stream);
+    if (st) {
+        // the array's address is per device: the stream must run on the current one
+        int cur = 0, sdev = 0;
+        cudaError_t e = cudaGetDevice(&cur);
+        if (e == cudaSuccess) e = cudaStreamGetDevice(st, &sdev);
+        if (e != cudaSuccess)
+            return fail(MSGB_ERR_CUDA, "msgb_sum_fwd_f32_static: device of the stream: %s", cudaGetErrorString(e));
+        if (sdev != cur)
+            return fail(MSGB_ERR_ARG, "msgb_sum_fwd_f32_static: the stream belongs to device %d but device %d is current",
+                        sdev, cur);
+    }
     void *scratch = nullptr;
     if (int e = static_scratch_address(&scratch)) return e;
     Layout l;
@@ -1442,7 +1454,6 @@ extern "C" int msgb_sum_fwd_f32_static(const msgb_problem *prob, const msgb_beam
     // Only the persistent kernel's work counter must start at zero; run_fwd
     // clears it on the stream before the launch.  Everything else in the
     // scratch is written by this call's preparation kernels before it is read.
-    cudaStream_t st = as_stream(stream);
     char *ws = (char *)scratch;
     switch (prob->ndim) {
         case 1: return run_fwd<1, false>(prob, beams, opts, ws, l, out, st, traj_src<1>(nullptr, nullptr, 1, 1));

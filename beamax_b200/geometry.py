@@ -92,8 +92,14 @@ class Domain:
         return np.stack(self.generate_meshgrid()[0], axis=-1)
 
     def _eval(self, p):
+        from .utils.interp import GridInterpolant
+
         if p is None:
             return None
+        if isinstance(p, GridInterpolant):
+            nodes = p.sample_nodes(self.N, self.dx)
+            if nodes is not None:
+                return nodes
         arr = np.asarray(p(self.grid) if callable(p) else p, dtype=float)
         if arr.ndim == 0:
             arr = np.broadcast_to(arr, self.N)
@@ -103,7 +109,14 @@ class Domain:
 
     @property
     def sound_speed_array(self) -> np.ndarray:
-        return self._eval(self.c)
+        """c on the grid; evaluated once per sound-speed object (a 3D cubic
+        interpolant takes seconds to sample at 128^3 points)."""
+        cached = getattr(self, "_c_grid_cache", None)
+        if cached is not None and cached[0] is self.c:
+            return cached[1]
+        arr = self._eval(self.c)
+        self._c_grid_cache = (self.c, arr)
+        return arr
 
     @property
     def density_array(self):

@@ -564,24 +564,37 @@ class MSGBSolver:
 
         if not self.keep_trajectories or self._traj_owner is None:
             return None
+        self._traj_cache = None  # free the previous forward's records first
         size = per * chunks[-1][1] + 4096
-        if len(chunks) > 1:
-            free, _ = torch.cuda.mem_get_info(dev)
-            if free < size + (4 << 30):
-                return None
+        free, _ = torch.cuda.mem_get_info(dev)
+        if free < size + (4 << 30):
+            return None
         return torch.empty(size, dtype=torch.uint8, device=dev)
 
+    def _propagation_key(self, domain):
+        """What the kept records depend on besides the selection and the time
+        grid: the medium object and absorption, the integrator settings and
+        the surrogate."""
+        kind, m = domain.medium()
+        return (kind, float(m) if kind == "constant" else id(m), float(domain.lam), repr(self.ode_config),
+                self.rk4_substeps, id(self.surrogate))
+
     def _remember_trajectories(self, buf, tr, domain, ts, nt):
+        """Keep the forward's last chunk of records (they stay on the device
+        until the next forward of this solver) for an adjoint with the same
+        selection, domain, time grid and propagation settings."""
         if buf is None:
             self._traj_cache = None
             return
+        tr.status = None  # the forward's status array is not kept
         self._traj_cache = {"selection": self._traj_owner, "domain": domain, "ts": ts, "nt": nt,
-                            "precision": self.precision, "tr": tr, "buf": buf}
+                            "precision": self.precision, "tr": tr, "buf": buf,
+                            "key": self._propagation_key(domain)}
 
     def _cached_trajectories(self, selection, domain, ts):
         c = self._traj_cache
         if (c is not None and c["selection"] is selection and c["domain"] is domain and c["ts"] is ts
-                and c["precision"] == self.precision):
+                and c["precision"] == self.precision and c["key"] == self._propagation_key(domain)):
             return c
         return None
 

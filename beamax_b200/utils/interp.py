@@ -76,6 +76,25 @@ class GridInterpolant:
     def ndim(self) -> int:
         return self.coeffs.ndim
 
+    def sample_nodes(self, N, dx):
+        """Values at the grid nodes k * dx (k = 0 .. N - 1) when those are the
+        interpolant's own nodes, else None.  At a node the cubic B-spline
+        weights are (1, 4, 1) / 6 and the linear ones (0, 1), so the samples
+        are a separable 3-tap filter of the coefficients (same boundary
+        rule): O(N) instead of 4^d taps per point."""
+        from scipy import ndimage
+
+        if (tuple(self.coeffs.shape) != tuple(N) or np.any(self.origin != 0.0)
+                or np.any(self.spacing != np.asarray(dx, dtype=float))):
+            return None
+        if self.method == "linear":
+            return self.coeffs.copy()
+        out = self.coeffs
+        for ax in range(self.ndim):
+            if out.shape[ax] > 1:
+                out = ndimage.correlate1d(out, np.array([1.0, 4.0, 1.0]) / 6.0, axis=ax, mode=self.boundary)
+        return out
+
     def _map(self, idx, n):
         if n == 1:
             return np.zeros_like(idx)

@@ -159,7 +159,7 @@ def config3(seed=0, thr=262144):
                          f"(4,8,16,32), four-sided sensor, thr={thr}, adaptive ODE")
 
 
-def config5(seed=0, thr=262144):
+def config5(seed=0, thr=262144, n_packets=512):
     """3D 128^3, dx 1e-4, c = 1500 (1 + 0.05 g) with a 20-cell correlation
     length, 3 levels (4, 8, 16) per axis, 512 packets + 16 blobs (sigma 6
     cells), planar sensor on the z = 0 face (128 x 128)."""
@@ -173,7 +173,7 @@ def config5(seed=0, thr=262144):
     mask[:, :, 0] = 1
     sensors = bb.Sensor(dom, binary_mask=mask)
     ts = dom.generate_time_domain()
-    p0 = make_p0(N, (4, 8, 16), 512, 16, 6.0, seed)
+    p0 = make_p0(N, (4, 8, 16), n_packets, 16, 6.0, seed)
     return dict(name=f"config5: 3D 128^3, c = 1500 (1 + 0.05 g), 20-cell correlation, 3 levels (4,8,16), "
                      f"planar z=0 sensor 128x128, thr={thr}, adaptive ODE",
                 domain=dom, wpt=wpt, sensors=sensors, ts=ts, p0=p0, thr=thr, hetero=True)
@@ -416,6 +416,59 @@ def run_ours(args, rank, world, device):
     return result
 
 
+def run_ode_only(args, device, peaks):
+    """The beam ODE alone (``--ode-only``): the workload's selection, then
+    msgb_ode_trajectories over every beam (both modes) writing the FP32
+    summation records and culling boxes, in the chunks the solver uses; W
+    untimed and K timed integrations, CUDA events on the launching stream."""
+    import torch
+
+    import beamax_b200 as bb
+
+    torch.cuda.set_device(device)
+    W = WORKLOADS[args.workload](seed=1234, thr=args.thr)
+    if not W["hetero"]:
+        raise SystemExit("--ode-only needs a heterogeneous workload (het512, c3, c5)")
+    dom, wpt, sens, ts, p0 = W["domain"], W["wpt"], W["sensors"], W["ts"], W["p0"]
+    s = bb.MSGBSolver(W["thr"], "top_n", 128, "spatial", bb.gb.gb_solvers.solve_ODE_base, "scan_real",
+                      precision="fp32")
+    sel = s.select(torch.from_numpy(p0).to(device), dom, wpt)
+    bt = s.beams(sel, dom, wpt)
+    pr, keep = s._problem(dom, sens, ts, device)
+    med, keep_m = s._medium(dom, device)
+    bs = bt.beam_set(unit=False)
+    st = torch.cuda.current_stream(device)
+    chunks, per, n_tt = s._mode_chunks(dom, pr.nt, bt, False)
+    status = torch.zeros(2 * bt.n, dtype=torch.int32, device=device)
+    ctr = torch.zeros(1, dtype=torch.int64, device=device)
+
+    def integrate():
+        for b_first, nb in chunks:
+            s._trajectories(pr, med, bs, b_first, nb, False, per, n_tt, device, st.cuda_stream, status)
+
+    for _ in range(max(args.warmup, 1)):
+        integrate()
+    torch.cuda.synchronize(device)
+    s.ode_step_counter = ctr
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    for _ in range(args.steps):
+        integrate()
+    b.record(st)
+    torch.cuda.synchronize(device)
+    secs = a.elapsed_time(b) / 1e3 / args.steps
+    steps = int(ctr.item()) / args.steps
+    fl = ode_flops_per_step(len(dom.N))
+    achieved = steps * fl / secs / 1e12
+    line = {"mode": "ode_only", "workload": W["name"], "beams": 2 * bt.n, "nt": pr.nt, "chunks": len(chunks),
+            "ode_s": secs, "attempted_steps": steps, "steps_per_beam": steps / (2 * bt.n),
+            "beam_steps_per_s": steps / secs, "flops_per_step": fl, "achieved_tflops": achieved,
+            "peak_fp64_tflops": peaks["fp64"] if peaks else None,
+            "frac": achieved / peaks["fp64"] if peaks else None, "status_max": int(status.max().item())}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def rooflines(r, peaks, sm_mhz, args):
     """Rooflines of the step's kernels, the one with the largest device time
     per step first (``roofline``), the others after it (``roofline_other``).
@@ -551,6 +604,7 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-peaks", action="store_true")
+    ap.add_argument("--ode-only", action="store_true", help="time the beam ODE alone (heterogeneous workloads)")
     args = ap.parse_args()
     if args.thr is None:
         args.thr = DEFAULT_THR[args.workload]
@@ -581,6 +635,8 @@ def main():
     device = torch.device("cuda", local_rank)
     torch.cuda.set_device(device)
     peaks = None if args.no_peaks else measure_peaks(device)
+    if args.ode_only:
+        return run_ode_only(args, device, peaks)
     r = run_ours(args, rank, world, device)
     if world > 1:
         torch.distributed.destroy_process_group()

@@ -135,7 +135,8 @@ int msgb_sum_fwd_f32(const msgb_problem *prob, const msgb_beam_set *beams,
  *     coefficients at that sensor count).
  *   - The first call on each device, with that device current, looks up the
  *     array's device address (cudaGetSymbolAddress); make that first call
- *     before any stream capture.
+ *     before any stream capture.  The stream must belong to the current
+ *     device (checked: MSGB_ERR_ARG otherwise).
  *   - Every call shares the one array, which keeps the last call's contents
  *     (the call clears what must start at zero).  Calls whose executions
  *     overlap on the GPU (different streams, or concurrent host threads)

@@ -52,6 +52,11 @@ def mT_inverse(xT, pT, mT_spc_time, mode, speed):
     B = mT_spc_time[0, 1:]
     C = mT_spc_time[1:, 1:]
     xs, ps = xdot[1:], pdot[1:]
+    if xdot[0] == 0.0:
+        # grazing beam (no velocity across the detector plane): the spatial
+        # Hessian is undefined; the caller replaces it with the reference's
+        # safe value i I (tr_solver_utils.py:424-435), as for p_n = 0
+        return 1j * np.eye(d)
     upper_right = (ps - C @ xs - B) / xdot[0]
     num = A + pdot[0] * xdot[0] - ps @ xs + xs @ C @ xs + 2 * (B @ xs)
     M = np.zeros((d, d), complex)

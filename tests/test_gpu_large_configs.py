@@ -142,9 +142,8 @@ def test_config5_full_geometry_matches_oracle():
 
     import beamax_b200 as bb
 
-    W = bench.config5(seed=1234)
     # fewer packets than the benchmark's 512 keep the host set-up short; the
     # grid, tiling, medium, sensor and thr are configuration 5's
-    W["p0"] = bench.make_p0(W["domain"].N, (4, 8, 16), 64, 16, 6.0, 1234)
+    W = bench.config5(seed=1234, n_packets=64)
     assert isinstance(W["sensors"], bb.Sensor)
     _run(W, False, 1024, 1e-6)

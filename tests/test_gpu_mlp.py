@@ -35,8 +35,12 @@ def gemm(A, B, bias=None, act=0, transA=False, transB=False):
     return C32, C16
 
 
+# K-contiguous operands run the TMA-fed persistent kernel (the larger cases
+# give every CTA several tiles: the A ring and both TMEM accumulators wrap);
+# transposed operands run the element-staging kernel.
 @pytest.mark.parametrize("M,N,K", [(128, 256, 256), (300, 256, 64), (128, 16, 256), (1000, 128, 16),
-                                   (256, 64, 200), (4096, 256, 256)])
+                                   (256, 64, 200), (4096, 256, 256), (56909, 256, 256), (20000, 16, 8),
+                                   (5000, 48, 256)])
 def test_gemm_matches_fp64_reference(M, N, K):
     dev = _dev()
     g = torch.Generator(device="cpu").manual_seed(M * 7 + N + K)

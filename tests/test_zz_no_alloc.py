@@ -116,3 +116,27 @@ def test_static_scratch_rejects_problems_beyond_its_size():
     assert "static scratch" in msg and str(STATIC_BYTES) in msg
     got = _static(pr, bs, opts)
     assert om.rel_l2(_with_workspace(pr, bs, opts).astype(np.float64), got.astype(np.float64)) < 1e-6
+
+
+def test_static_scratch_forward_allocates_no_device_memory():
+    """After a warm-up call (module load, symbol lookup), a further call leaves
+    the device's free memory and torch's allocated bytes unchanged: the entry
+    point takes its scratch from the array, not from an allocator."""
+    from beamax_b200 import _lib
+
+    dev = _dev()
+    pr, bs, opts, keep = _case((128, 128), 1500, 0, interior_sensors=False)
+    out = torch.empty((pr.nt, pr.ns), dtype=torch.float32, device=dev)
+    st = torch.cuda.current_stream().cuda_stream
+    call = lambda: _lib.check(_lib.lib().msgb_sum_fwd_f32_static(_lib.ref(pr), _lib.ref(bs), _lib.ref(opts),
+                                                                  out.data_ptr(), st), "msgb_sum_fwd_f32_static")
+    call()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(dev)
+    alloc0 = torch.cuda.memory_allocated(dev)
+    call()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(dev)
+    assert free1 == free0
+    assert torch.cuda.memory_allocated(dev) == alloc0
+    assert np.isfinite(out.cpu().numpy()).all()
