@@ -1214,6 +1214,8 @@ int run_adj(const msgb_problem *p, const msgb_beam_set *b, const msgb_sum_opts *
     const unsigned grid = (unsigned)(want < n_items ? want : n_items);
     const size_t smem = (size_t)NACC * 2 * sizeof(double);
     auto args = [&](auto kern) {
+        // static + dynamic shared memory exceed the default 48 KB: opt in
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         kern<<<grid, THREADS, smem, st>>>(P, to_args(b), (const Cull<D> *)(ws + l.cull),
                                           (const TileInfo<D> *)(ws + l.tiles), (const int32_t *)(ws + l.offs),
                                           (const float *)(ws + l.ds), (const float *)(ws + l.hn),

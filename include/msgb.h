@@ -510,8 +510,10 @@ int msgb_tr_final_states(const msgb_problem *prob, const msgb_medium *med, const
 
 /* ---- adjoint scatter to coefficient space ------------------------------ */
 
-/* G[idx[j]] += scale * g[j] for unique idx (no atomics needed); G must be
- * zeroed by the caller.  Complex FP64. */
+/* G[idx[j]] += scale * g[j]; G must be zeroed by the caller.  Complex FP64.
+ * Precondition: the n indices are distinct (a selection of top_n or of a
+ * threshold always is).  Each entry is updated by one thread without atomics,
+ * so duplicate indices race and leave G undefined at those entries. */
 int msgb_scatter_coeff_grad(const int64_t *idx, const double *g, int64_t n, double scale,
                             const msgb_mswpt *plan, int apply_half_mask, double *G,
                             msgb_stream_t stream);
