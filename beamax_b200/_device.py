@@ -50,6 +50,9 @@ def workspace(device, name: str, nbytes: int):
     with _ws_lock:
         buf = _workspaces.get(key)
         if buf is None or buf.numel() < nbytes:
+            # release the smaller buffer before allocating the larger one
+            _workspaces.pop(key, None)
+            buf = None
             buf = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=dev)
             _workspaces[key] = buf
     assert buf.data_ptr() % 256 == 0

@@ -72,7 +72,8 @@ class SurrogateAccept(ctypes.Structure):
 
 class Trajectories(ctypes.Structure):
     _fields_ = [("nb", c_i64), ("b_first", c_i64), ("rec64", c_vp), ("rec32", c_vp), ("cull", c_vp),
-                ("status", c_vp)]
+                ("status", c_vp), ("slot", c_vp), ("pool", c_vp), ("pool_cull", c_vp), ("pool_blocks", c_i64),
+                ("pool_next", c_vp), ("live_boxes", c_vp), ("n_boxes", c_i64), ("live_cutoff", c_dbl)]
 
 
 class Gemm(ctypes.Structure):
@@ -145,6 +146,8 @@ SIGNATURES = {
     "msgb_tr_final_states": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "msgb_scatter_coeff_grad": (ctypes.c_int, [c_vp, c_vp, c_i64, c_dbl, c_vp, ctypes.c_int,
                                                 c_vp, c_vp]),
+    "msgb_sum_f32_tile_count": (c_i64, [c_vp, c_vp]),
+    "msgb_sum_f32_tile_boxes": (ctypes.c_int, [c_vp, c_vp, c_vp, c_sz, c_vp, c_vp]),
     "msgb_peak_probe_ops": (c_dbl, [ctypes.c_int, c_i64, ctypes.c_int, ctypes.c_int]),
     "msgb_peak_probe": (ctypes.c_int, [ctypes.c_int, c_i64, ctypes.c_int, ctypes.c_int, c_vp, c_vp]),
 }

@@ -721,7 +721,9 @@ extern "C" int msgb_ode_trajectories(const msgb_problem *prob, const msgb_medium
     ProbArgs P = to_args(prob);
     OdeArgs O{opts->method, opts->substeps, opts->rtol, opts->atol, opts->dt0, opts->max_steps, opts->only_flagged,
               opts->dense_output, opts->step_count};
+    if (int e = check_compact(out, prob->ndim)) return e;
     TrajArgs T{out->nb, out->b_first, beams->n, out->rec64, out->rec32, out->cull, out->status};
+    set_compact(T, out);
     const int blk = 64;
     const int64_t need = (out->nb + blk - 1) / blk;
     cudaStream_t st = as_stream(stream);

@@ -516,8 +516,11 @@ __global__ void transpose_permute_kernel(const float *data, const int32_t *perm,
 template <int D>
 struct TrajSrc {
     int64_t nb, b_first;
-    const BeamTime<D> *rec;   // (nt, nb)
-    const float *cull;        // (n_tt, nb, 2D + 1)
+    const BeamTime<D> *rec;   // dense: (nt, nb)
+    const float *cull;        // dense: (n_tt, nb, 2D + 1)
+    const int32_t *slot;      // compact: (n_tt, nb) block or -1
+    const BeamTime<D> *pool;  // compact: (blocks, TT)
+    const float *pool_cull;   // compact: (blocks, 2D + 1)
     float *state;             // (2, nt, ns) Kahan sum / compensation, sorted sensor order
     int first, last;
 };
@@ -525,8 +528,16 @@ struct TrajSrc {
 template <int D>
 __device__ __forceinline__ bool traj_survives(const TrajSrc<D> &T, int64_t bl, int64_t tt, const TileInfo<D> &ti,
                                               float cutoff) {
-    if (cutoff <= 0.0f) return true;
-    const float *c = T.cull + (tt * T.nb + bl) * (2 * D + 1);
+    const float *c;
+    if (T.pool) {
+        const int32_t blk = T.slot[tt * T.nb + bl];
+        if (blk < 0) return false;  // no sensor tile within the cutoff: not stored
+        if (cutoff <= 0.0f) return true;
+        c = T.pool_cull + (int64_t)blk * (2 * D + 1);
+    } else {
+        if (cutoff <= 0.0f) return true;
+        c = T.cull + (tt * T.nb + bl) * (2 * D + 1);
+    }
     float d2 = 0.0f;
 #pragma unroll
     for (int i = 0; i < D; ++i) {
@@ -539,7 +550,10 @@ __device__ __forceinline__ bool traj_survives(const TrajSrc<D> &T, int64_t bl, i
 template <int D>
 __device__ __forceinline__ void traj_beam_time(const BeamArgs &B, const TrajSrc<D> &T, int64_t bl, int64_t k,
                                                BeamTime<D> &bt) {
-    bt = T.rec[k * T.nb + bl];
+    if (T.pool)
+        bt = T.pool[(int64_t)T.slot[(k / TT) * T.nb + bl] * TT + k % TT];
+    else
+        bt = T.rec[k * T.nb + bl];
     const int64_t b = T.b_first + bl;
     const int64_t j = b < B.n ? b : b - B.n;
     const double ar = B.a0[2 * j], ai = B.a0[2 * j + 1];
@@ -1242,6 +1256,11 @@ TrajSrc<D> traj_src(const msgb_trajectories *t, float *state, int first, int las
         T.b_first = t->b_first;
         T.rec = (const BeamTime<D> *)t->rec32;
         T.cull = t->cull;
+        if (t->pool) {
+            T.slot = t->slot;
+            T.pool = (const BeamTime<D> *)t->pool;
+            T.pool_cull = t->pool_cull;
+        }
     }
     T.state = state;
     T.first = first;
@@ -1330,8 +1349,12 @@ extern "C" size_t msgb_sum_f32_traj_workspace_size(const msgb_problem *prob, int
 // with_part: the adjoint's partials (n_tt, nb) follow the Kahan state.
 static int check_traj32(const msgb_problem *p, const msgb_beam_set *b, const msgb_trajectories *t,
                         const msgb_sum_opts *o, void *ws, size_t bytes, bool with_part, Layout &l) {
-    if (!t || !t->rec32) return fail(MSGB_ERR_ARG, "FP32 trajectory records are NULL");
-    if (!t->cull && o && o->cutoff > 0.0) return fail(MSGB_ERR_ARG, "culling boxes are NULL");
+    if (!t || (!t->rec32 && !t->pool)) return fail(MSGB_ERR_ARG, "FP32 trajectory records are NULL");
+    if (t->pool) {
+        if (!t->slot || !t->pool_cull) return fail(MSGB_ERR_ARG, "compact trajectories: slot or pool_cull is NULL");
+    } else if (!t->cull && o && o->cutoff > 0.0) {
+        return fail(MSGB_ERR_ARG, "culling boxes are NULL");
+    }
     if (t->nb < 0 || t->b_first < 0 || t->b_first + t->nb > 2 * b->n)
         return fail(MSGB_ERR_ARG, "trajectory beam range outside [0, 2n)");
     l = layout(p, 0, true, tile_count(p, o));
@@ -1383,6 +1406,56 @@ extern "C" int msgb_adj_gather_f32_traj(const msgb_problem *prob, const msgb_bea
         case 1: return run_adj<1, true>(prob, beams, opts, ws, l, data, part, g, st, traj_src<1>(traj, nullptr, 1, 1));
         case 2: return run_adj<2, true>(prob, beams, opts, ws, l, data, part, g, st, traj_src<2>(traj, nullptr, 1, 1));
         default: return run_adj<3, true>(prob, beams, opts, ws, l, data, part, g, st, traj_src<3>(traj, nullptr, 1, 1));
+    }
+}
+
+// ---- sensor-tile boxes (for the compact trajectory store) -------------------
+namespace msgb {
+namespace {
+template <int D>
+__global__ void tile_boxes_kernel(const TileInfo<D> *tiles, int64_t n_st, float *boxes) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n_st) return;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        boxes[i * 2 * D + a] = tiles[i].lo[a];
+        boxes[i * 2 * D + D + a] = tiles[i].hi[a];
+    }
+}
+
+template <int D>
+int tile_boxes(const msgb_problem *p, const msgb_sum_opts *o, char *ws, const Layout &l, float *boxes,
+               cudaStream_t st) {
+    msgb_beam_set none{};
+    if (int e = prep<D>(p, &none, o, l, ws, st)) return e;
+    tile_boxes_kernel<D><<<(unsigned)((l.n_st + 127) / 128), 128, 0, st>>>((const TileInfo<D> *)(ws + l.tiles),
+                                                                           l.n_st, boxes);
+    return check_launch("msgb_sum_f32_tile_boxes");
+}
+}  // namespace
+}  // namespace msgb
+
+extern "C" int64_t msgb_sum_f32_tile_count(const msgb_problem *prob, const msgb_sum_opts *opts) {
+    if (validate_problem(prob)) return -1;
+    return tile_count(prob, opts);
+}
+
+extern "C" int msgb_sum_f32_tile_boxes(const msgb_problem *prob, const msgb_sum_opts *opts, void *workspace,
+                                       size_t workspace_bytes, float *boxes, msgb_stream_t stream) {
+    if (int e = validate_problem(prob)) return e;
+    if (!boxes) return fail(MSGB_ERR_ARG, "msgb_sum_f32_tile_boxes: boxes is NULL");
+    if (prob->ns == 0) return MSGB_OK;
+    const Layout l = layout(prob, 0, true, tile_count(prob, opts));
+    if (l.n_st <= 0) return fail(MSGB_ERR_ARG, "sensor tiling has no tiles");
+    if (!workspace || workspace_bytes < l.total)
+        return fail(MSGB_ERR_WORKSPACE, "workspace too small: need %zu bytes, got %zu", l.total, workspace_bytes);
+    if (((uintptr_t)workspace & 255) != 0) return fail(MSGB_ERR_WORKSPACE, "workspace must be 256-byte aligned");
+    cudaStream_t st = as_stream(stream);
+    char *ws = (char *)workspace;
+    switch (prob->ndim) {
+        case 1: return tile_boxes<1>(prob, opts, ws, l, boxes, st);
+        case 2: return tile_boxes<2>(prob, opts, ws, l, boxes, st);
+        default: return tile_boxes<3>(prob, opts, ws, l, boxes, st);
     }
 }
 

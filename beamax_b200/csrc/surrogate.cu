@@ -346,6 +346,7 @@ extern "C" int msgb_surrogate_records(const msgb_problem *prob, const msgb_mediu
     if (io->b_first < out->b_first || io->b_first + io->nb > out->b_first + out->nb)
         return fail(MSGB_ERR_ARG, "predicted beams lie outside the trajectory chunk");
     if (S.nb == 0 || prob->nt == 0) return MSGB_OK;
+    if (out->pool) return fail(MSGB_ERR_UNSUPPORTED, "msgb_surrogate_records writes the dense FP32 layout (rec32)");
     AcceptArgs A{accept->residual_tol, accept->phase_tol, accept->pos_err};
     TrajArgs T{out->nb, out->b_first, beams->n, out->rec64, out->rec32, out->cull, out->status};
     const int blk = 64;

@@ -217,7 +217,40 @@ struct TrajArgs {
     void *rec32;
     float *cull;
     int32_t *status;
+    // compact FP32 store (pool != nullptr): see msgb_trajectories
+    int32_t *slot = nullptr;
+    void *pool = nullptr;
+    float *pool_cull = nullptr;
+    int64_t pool_blocks = 0;
+    unsigned long long *pool_next = nullptr;
+    const float *boxes = nullptr;
+    int64_t n_boxes = 0;
+    float live_cutoff = 0.0f;
 };
+
+// Host: the compact-store fields of a msgb_trajectories descriptor.
+inline void set_compact(TrajArgs &T, const msgb_trajectories *t) {
+    T.slot = t->slot;
+    T.pool = t->pool;
+    T.pool_cull = t->pool_cull;
+    T.pool_blocks = t->pool_blocks;
+    T.pool_next = t->pool_next;
+    T.boxes = t->live_boxes;
+    T.n_boxes = t->n_boxes;
+    T.live_cutoff = (float)t->live_cutoff;
+}
+
+inline int check_compact(const msgb_trajectories *t, int ndim) {
+    if (!t->pool) return MSGB_OK;
+    if (t->rec32) return fail(MSGB_ERR_ARG, "trajectories: rec32 and a compact pool are exclusive");
+    if (!t->slot || !t->pool_cull || !t->pool_next || t->pool_blocks < 1)
+        return fail(MSGB_ERR_ARG, "trajectories: compact store needs slot, pool_cull, pool_next and pool_blocks > 0");
+    if (t->n_boxes < 0 || (t->n_boxes > 0 && !t->live_boxes))
+        return fail(MSGB_ERR_ARG, "trajectories: live_boxes is NULL");
+    if (!(t->live_cutoff >= 0.0)) return fail(MSGB_ERR_ARG, "trajectories: live_cutoff must be >= 0");
+    (void)ndim;
+    return MSGB_OK;
+}
 
 
 // Writes the records of one beam (index bl within the chunk) at every time k,
@@ -234,6 +267,9 @@ struct RecordWriter {
     float lo[D], hi[D];
     double lmin = 1e300;
     bool bad = false;
+    // compact store: this lane's block for the current time tile (-1: none
+    // taken yet; kept across beams when a dead tile did not use it)
+    int64_t blk = -1;
 
     __device__ RecordWriter(const ProbArgs &P_, const TrajArgs &T_, int64_t bl_, double w_, int tt_len_)
         : P(P_), T(T_), bl(bl_), w(w_), tt_len(tt_len_) {
@@ -274,9 +310,18 @@ struct RecordWriter {
             r[q++] = y.A.re;
             r[q++] = y.A.im;
         }
-        if (T.rec32) {
+        const int kk_tile = (int)(k % tt_len);
+        char *rec32_base = nullptr;
+        if (T.pool) {
+            if (kk_tile == 0 && blk < 0) blk = (int64_t)atomicAdd(T.pool_next, 1ULL);
+            if (blk < T.pool_blocks)
+                rec32_base = (char *)T.pool + (blk * tt_len + kk_tile) * (int64_t)(16 * D + 8 * S + 8);
+        } else if (T.rec32) {
+            rec32_base = (char *)T.rec32 + (k * T.nb + bl) * (int64_t)(16 * D + 8 * S + 8);
+        }
+        if (rec32_base) {
             // layout of the FP32 summation's BeamTime<D> record
-            char *base = (char *)T.rec32 + (k * T.nb + bl) * (int64_t)(16 * D + 8 * S + 8);
+            char *base = rec32_base;
             double *xd = (double *)base;
             double *wpd = xd + D;
             float *f = (float *)(wpd + D);
@@ -302,7 +347,7 @@ struct RecordWriter {
             f[2 * S] = atan2f(aim, (are == 0.0f && aim == 0.0f) ? 1e-12f : are);
             f[2 * S + 1] = 2.0f * hypotf(are, aim);
         }
-        if (T.cull) {
+        if (T.cull || T.pool) {
             double Sm[D][D];
 #pragma unroll
             for (int i = 0; i < D; ++i)
@@ -322,15 +367,45 @@ struct RecordWriter {
                 hi[i] = fmaxf(hi[i], xf);
             }
             if (kk == tt_len - 1 || k == P.nt - 1) {
-                float *c = T.cull + ((k / tt_len) * T.nb + bl) * (2 * D + 1);
+                float box[2 * D + 1];
 #pragma unroll
                 for (int i = 0; i < D; ++i) {
                     // periodic axes and non-finite states are never culled
                     const bool open = P.periodic[i] || bad;
-                    c[i] = open ? -3.4e38f : lo[i];
-                    c[D + i] = open ? 3.4e38f : hi[i];
+                    box[i] = open ? -3.4e38f : lo[i];
+                    box[D + i] = open ? 3.4e38f : hi[i];
                 }
-                c[2 * D] = bad ? 0.0f : (float)fmax(0.0, 0.5 * w * lmin * (1.0 - 1e-6));
+                box[2 * D] = bad ? 0.0f : (float)fmax(0.0, 0.5 * w * lmin * (1.0 - 1e-6));
+                if (T.pool) {
+                    // live: within the cutoff of some sensor tile (the summation's
+                    // own test, with the cutoff widened by 1e-4 so that every
+                    // tile the summation keeps is stored)
+                    bool live = bad || T.n_boxes == 0;
+                    for (int64_t q = 0; q < T.n_boxes && !live; ++q) {
+                        const float *tb = T.boxes + q * 2 * D;
+                        float d2 = 0.0f;
+#pragma unroll
+                        for (int i = 0; i < D; ++i) {
+                            const float gap = fmaxf(0.0f, fmaxf(tb[i] - box[D + i], box[i] - tb[D + i]));
+                            d2 = fmaf(gap, gap, d2);
+                        }
+                        live = box[2 * D] * d2 * 0.999f <= T.live_cutoff * 1.0001f;
+                    }
+                    int32_t *sl = T.slot + (k / tt_len) * T.nb + bl;
+                    if (live && blk >= 0 && blk < T.pool_blocks) {
+                        *sl = (int32_t)blk;
+                        float *c = T.pool_cull + blk * (2 * D + 1);
+#pragma unroll
+                        for (int i = 0; i < 2 * D + 1; ++i) c[i] = box[i];
+                        blk = -1;  // the block belongs to this tile now
+                    } else {
+                        *sl = -1;  // dead tile (or pool exhausted): the block is reused
+                    }
+                } else {
+                    float *c = T.cull + ((k / tt_len) * T.nb + bl) * (2 * D + 1);
+#pragma unroll
+                    for (int i = 0; i < 2 * D + 1; ++i) c[i] = box[i];
+                }
             }
         }
     }

@@ -120,8 +120,12 @@ class MSGBSolver:
         a (beam, time tile, sensor tile) triple.
       rk4_substeps: RK4 steps per save interval when ``ode_config.solver`` is
         "rk4" (overrides ``ode_config.substeps`` when > 1).
-      trajectory_memory: bytes of device memory for trajectory records; beams
-        are propagated and summed in chunks that fit.
+      trajectory_memory: bytes of device memory for trajectory records (at
+        most what the device has free less 4 GiB); beams are propagated and
+        summed in chunks that fit.  The FP32 path stores a (time tile, beam)
+        block of records only when it comes within the cutoff of a sensor
+        tile (a compact store, typically 35-40 % of the tiles at the
+        configuration-3 geometry), so far more beams fit per chunk.
       surrogate: a fitted ``beamax_b200.surrogate.TrajectorySurrogate`` for the
         medium and time grid; heterogeneous beams are predicted by it and the
         ones it does not accept are integrated.
@@ -130,12 +134,15 @@ class MSGBSolver:
         selection, domain and time grid does not integrate those beams again:
         all of them when they fit in trajectory_memory, else the last chunk
         of beams (when the device has room for it beside the chunk buffer).
+      compact_trajectories: the FP32 path's compact record store (default);
+        False stores every (time, beam) record (the same results, more memory).
     """
 
     def __init__(self, thr, thr_strat: str, batch_size: int, input_type: str, ode_solver, sum_method: str,
                  tr_ode_solver=None, sharding=None, ode_config=None, adjoint_relative_guard: float = 5e-2,
                  *, precision: str = "fp64", cutoff: float = 16.0, rk4_substeps: int = 1,
-                 trajectory_memory: int = 48 << 30, surrogate=None, keep_trajectories: bool = True):
+                 trajectory_memory: int = 96 << 30, surrogate=None, keep_trajectories: bool = True,
+                 compact_trajectories: bool = True):
         valid_thresholds = {"hard", "top_n", "percentile", "hard_reassign", "bao_energy", "perc_max_abs"}
         if thr_strat not in valid_thresholds:
             raise ValueError(f"thr_strat must be one of {', '.join(sorted(valid_thresholds))}; got {thr_strat!r}.")
@@ -196,8 +203,11 @@ class MSGBSolver:
         self.trajectory_memory = int(trajectory_memory)
         self.surrogate = surrogate
         self.keep_trajectories = bool(keep_trajectories)
+        self.compact_trajectories = bool(compact_trajectories)
         self._traj_cache = None
         self._traj_owner = None
+        self._live_est = 0.5  # fraction of (time tile, beam) pairs the compact store keeps
+        self._compact_kept = None
         # When set to a list, every FP32 summation entry point call appends
         # (name, start event, end event, evaluation counter) recorded on the
         # launching stream around the call.
@@ -429,12 +439,12 @@ class MSGBSolver:
         reference's do)."""
         return not self.closed_form and self.heterogeneous(domain)
 
-    def _chunks(self, domain: Domain, nt: int, nbeam: int, fp64: bool):
+    def _chunks(self, domain: Domain, nt: int, nbeam: int, fp64: bool, budget: Optional[int] = None):
         d = domain.ndim
         S = d * (d + 1) // 2
         n_tt = (nt + 31) // 32
         per = nt * ((2 * d + 2 * d * d + 2) * 8 if fp64 else (16 * d + 8 * S + 8)) + n_tt * (2 * d + 1) * 4
-        chunk = max(1, min(nbeam, self.trajectory_memory // max(per, 1)))
+        chunk = max(1, min(nbeam, (budget or self.trajectory_memory) // max(per, 1)))
         return [(b, min(chunk, nbeam - b)) for b in range(0, nbeam, chunk)], per, n_tt
 
     def _ode_opts(self, ts):
@@ -450,7 +460,7 @@ class MSGBSolver:
         +1 only) or [n, 2n) (mode -1 only)."""
         n = bt.n
         lo, hi = {0: (0, 2 * n), 1: (0, n), 2: (n, 2 * n)}[bt.modes]
-        chunks, per, n_tt = self._chunks(domain, nt, hi - lo, fp64)
+        chunks, per, n_tt = self._chunks(domain, nt, hi - lo, fp64, self._trajectory_budget(bt.x0.device))
         return [(lo + b, nb) for b, nb in chunks], per, n_tt
 
     def _trajectories(self, pr, med, bs, b_first, nb, fp64, per, n_tt, dev, st, status, buf=None):
@@ -476,6 +486,128 @@ class MSGBSolver:
             _lib.check(_lib.lib().msgb_ode_trajectories(_lib.ref(pr), _lib.ref(med), _lib.ref(bs), _lib.ref(opts),
                                                         _lib.ref(tr), st), "msgb_ode_trajectories")
         return tr, buf
+
+    # ---- compact FP32 trajectory store -----------------------------------
+    def _compact(self) -> bool:
+        """FP32 records are kept only for (time tile, beam) pairs within the
+        cutoff of some sensor tile (the summation skips the others anyway)."""
+        return (self.compact_trajectories and self.precision == "fp32" and self.surrogate is None
+                and self.cutoff > 0)
+
+    def _live_boxes(self, pr, opts, domain, sensors, dev, st):
+        """The summation's sensor-tile boxes (n_tiles, 2 d) on the device."""
+        import torch
+
+        def make():
+            n = int(_lib.lib().msgb_sum_f32_tile_count(_lib.ref(pr), _lib.ref(opts)))
+            nbytes = _lib.lib().msgb_sum_f32_traj_workspace_size(_lib.ref(pr), 0)
+            ws = workspace(dev, "sum32traj", nbytes)
+            boxes = torch.empty((max(n, 1), 2 * pr.ndim), dtype=torch.float32, device=dev)
+            _lib.check(_lib.lib().msgb_sum_f32_tile_boxes(_lib.ref(pr), _lib.ref(opts), ws.data_ptr(), nbytes,
+                                                          boxes.data_ptr(), st), "msgb_sum_f32_tile_boxes")
+            return boxes, n
+
+        if isinstance(sensors, Sensor):
+            return _cache.get(sensors, ("live_boxes", str(dev), tuple(domain.dx), pr.nt), make)
+        return make()
+
+    @staticmethod
+    def _compact_sizes(d: int, nt: int):
+        S = d * (d + 1) // 2
+        n_tt = (nt + 31) // 32
+        block = 32 * (16 * d + 8 * S + 8)          # one time tile of FP32 records
+        cull = (2 * d + 1) * 4
+        return n_tt, block, cull
+
+    def _trajectory_budget(self, dev) -> int:
+        """Bytes for one chunk of trajectory records: trajectory_memory, or
+        what the device has free less 4 GiB of headroom."""
+        import torch
+
+        free, _ = torch.cuda.mem_get_info(dev)
+        return int(max(1 << 20, min(self.trajectory_memory, free - (4 << 30))))
+
+    def _compact_chunk_beams(self, d, nt, nbeam, budget):
+        """Beams per chunk for the estimated fraction of live tiles (each beam
+        may also leave one block that no live tile took)."""
+        n_tt, block, cull = self._compact_sizes(d, nt)
+        per_beam = n_tt * 4 + self._live_est * n_tt * (block + cull) + (block + cull)
+        return int(max(1, min(nbeam, (budget - 4096) // max(per_beam, 1))))
+
+    def _compact_tr(self, buf, d, nt, b_first, nb, status, boxes, n_boxes):
+        """Lay out the slot table, counter, culling boxes and record blocks of
+        one chunk in buf; returns (Trajectories, blocks, counter view)."""
+        n_tt, block, cull = self._compact_sizes(d, nt)
+        base = buf.data_ptr()
+        al = lambda x: (x + 255) // 256 * 256
+        slot_b = al(n_tt * nb * 4)
+        ctr_off = slot_b
+        rest = buf.numel() - slot_b - 512
+        blocks = max(0, rest // (block + cull) - 2)
+        cull_off = slot_b + 256
+        pool_off = al(cull_off + blocks * cull)
+        blocks = max(0, min(blocks, (buf.numel() - pool_off) // block))
+        tr = _lib.Trajectories(nb=nb, b_first=b_first, status=status.data_ptr() + 4 * b_first,
+                               slot=base, pool=base + pool_off, pool_cull=base + cull_off, pool_blocks=blocks,
+                               pool_next=base + ctr_off, live_boxes=boxes.data_ptr(), n_boxes=n_boxes,
+                               live_cutoff=float(self.cutoff))
+        ctr = buf[ctr_off:ctr_off + 8].view(dtype=__import__("torch").int64)
+        return tr, blocks, ctr
+
+    def _compact_integrate(self, pr, med, bs, lo, hi, domain, sensors, opts, dev, st, status, keep=False,
+                           skip=None):
+        """Integrate beams [lo, hi) into compact chunks, yielding (tr, first,
+        last) per chunk in beam order.  A chunk whose pool runs out (more live
+        tiles than estimated) is split in two and integrated again.  skip:
+        (b_first, nb) of a chunk the caller already holds (not integrated).
+        keep: the buffer of the last chunk is returned in self._compact_kept."""
+        import torch
+
+        d = pr.ndim
+        n_tt, block, cull = self._compact_sizes(d, pr.nt)
+        boxes, n_boxes = self._live_boxes(pr, opts, domain, sensors, dev, st)
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        lanes = 4 * sms * 64  # the integrator's resident lanes
+        todo = []
+        ranges = [(lo, hi)] if skip is None else [(lo, skip[0]), (skip[0] + skip[1], hi)]
+        budget = self._trajectory_budget(dev)
+        cb = 1
+        for a, b in ranges:
+            if b <= a:
+                continue
+            cb = self._compact_chunk_beams(d, pr.nt, b - a, budget)
+            todo += [(x, min(cb, b - x)) for x in range(a, b, cb)]
+        if not todo:
+            return
+        # the chunk's estimated need (plus one block per integrator lane), not the whole budget
+        widest = max(nb for _, nb in todo)
+        need = int(widest * n_tt * (4 + self._live_est * (block + cull)) + min(widest, lanes) * (block + cull)
+                   + 4096)
+        buf = torch.empty(min(budget, need), dtype=torch.uint8, device=dev)
+        first = True
+        opts_ode = self._ode_opts(None)
+        if self.ode_step_counter is not None:
+            opts_ode.step_count = self.ode_step_counter.data_ptr()
+        while todo:
+            b_first, nb = todo.pop(0)
+            tr, blocks, ctr = self._compact_tr(buf, d, pr.nt, b_first, nb, status, boxes, n_boxes)
+            ctr.zero_()
+            with self._kernel_span("msgb_ode_trajectories", None):
+                _lib.check(_lib.lib().msgb_ode_trajectories(_lib.ref(pr), _lib.ref(med), _lib.ref(bs),
+                                                            _lib.ref(opts_ode), _lib.ref(tr), st),
+                           "msgb_ode_trajectories")
+            used = int(ctr.item())
+            if used > blocks:
+                if nb == 1:
+                    raise RuntimeError("compact trajectory store: one beam needs more than the budget")
+                self._live_est = min(1.0, self._live_est * 2.0)
+                todo[:0] = [(b_first, nb // 2), (b_first + nb // 2, nb - nb // 2)]
+                continue
+            self._live_est = min(1.0, max(0.05, 1.15 * max(0, used - min(nb, lanes)) / max(1, n_tt * nb)))
+            if keep and not todo:
+                self._compact_kept = buf
+            yield tr, first, not todo
+            first = False
 
     def _begin_trajectories(self, domain, ts):
         self._accepted = None
@@ -523,7 +655,7 @@ class MSGBSolver:
         status = torch.zeros(2 * bt.n, dtype=torch.int32, device=dev)
         self._begin_trajectories(domain, ts)
         self._traj_cache = None
-        keep_buf = self._keep_buffer(chunks, per, dev)
+        keep_buf = None if (not fp64 and self._compact()) else self._keep_buffer(chunks, per, dev)
         last = len(chunks) - 1
         if fp64:
             out = torch.zeros((pr.nt, pr.ns), dtype=torch.float64, device=dev)
@@ -540,6 +672,24 @@ class MSGBSolver:
         tiling = self._tiling(domain, sensors, dev)
         opts = _lib.SumOpts(cutoff=self.cutoff, eval_count=cnt.data_ptr(),
                             tiling=_lib.ref(tiling[0]) if tiling else None)
+        if self._compact():
+            keep_buf = None  # the compact path keeps its own last chunk
+            lo, hi = chunks[0][0], chunks[-1][0] + chunks[-1][1]
+            keep = self.keep_trajectories and self._traj_owner is not None
+            self._compact_kept = None
+            for tr, first, last in self._compact_integrate(pr, med, bs, lo, hi, domain, sensors, opts, dev, st,
+                                                          status, keep=keep):
+                nbytes = _lib.lib().msgb_sum_f32_traj_workspace_size(_lib.ref(pr), tr.nb)
+                ws = workspace(dev, "sum32traj", nbytes)
+                with self._kernel_span("msgb_sum_fwd_f32_traj", cnt):
+                    _lib.check(_lib.lib().msgb_sum_fwd_f32_traj(_lib.ref(pr), _lib.ref(bs), _lib.ref(tr),
+                                                                _lib.ref(opts), int(first), int(last), ws.data_ptr(),
+                                                                nbytes, out.data_ptr(), st), "msgb_sum_fwd_f32_traj")
+            self._eval_counter = cnt
+            self._check_status(status)
+            self._remember_trajectories(self._compact_kept, tr, domain, ts, pr.nt)
+            self._compact_kept = None
+            return out
         nbytes = _lib.lib().msgb_sum_f32_traj_workspace_size(_lib.ref(pr), max(nb for _, nb in chunks))
         ws = workspace(dev, "sum32traj", nbytes)
         for i, (b_first, nb) in enumerate(chunks):
@@ -625,6 +775,25 @@ class MSGBSolver:
         status = torch.zeros(2 * n, dtype=torch.int32, device=dev)
         self._begin_trajectories(domain, ts)
         kept = (cached["tr"].b_first, cached["tr"].nb) if cached is not None else None
+        if not fp64 and self._compact():
+            lo, hi = chunks[0][0], chunks[-1][0] + chunks[-1][1]
+            trs = []
+            if kept is not None and lo <= kept[0] and kept[0] + kept[1] <= hi:
+                trs.append(cached["tr"])  # the forward's records for these beams
+            else:
+                kept = None
+            gen = self._compact_integrate(pr, med, bs, lo, hi, domain, sensors, opts, dev, st, status, skip=kept)
+            for tr in _chain(trs, (t for t, _, _ in gen)):
+                nbytes = _lib.lib().msgb_sum_f32_traj_workspace_size(_lib.ref(pr), tr.nb)
+                ws = workspace(dev, "sum32traj", nbytes)
+                gp = torch.view_as_real(g_all[tr.b_first:tr.b_first + tr.nb]).data_ptr()
+                with self._kernel_span("msgb_adj_gather_f32_traj", cnt):
+                    _lib.check(_lib.lib().msgb_adj_gather_f32_traj(_lib.ref(pr), _lib.ref(bs), _lib.ref(tr),
+                                                                   _lib.ref(opts), ws.data_ptr(), nbytes,
+                                                                   d.data_ptr(), gp, st), "msgb_adj_gather_f32_traj")
+            self._eval_counter = cnt
+            self._check_status(status)
+            return g_all[:n] + g_all[n:]
         for b_first, nb in chunks:
             if (b_first, nb) == kept:
                 tr = cached["tr"]  # the forward's records for these beams, in this order
@@ -1166,6 +1335,11 @@ class MSGBSolver:
         """Evaluated (beam, time, sensor) triples of the last FP32 call."""
         c = getattr(self, "_eval_counter", None)
         return None if c is None else int(c.item())
+
+
+def _chain(*its):
+    for it in its:
+        yield from it
 
 
 def torch_argsort(x):

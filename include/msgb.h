@@ -201,6 +201,28 @@ typedef struct msgb_trajectories {
     void *rec32;
     float *cull;
     int32_t *status;
+    /* Compact FP32 store (used when rec32 is NULL and pool is not): records of
+     * a (time tile, beam) pair are kept only when its culling box comes within
+     * `live_cutoff` e-folds of at least one of the `n_boxes` sensor-tile boxes
+     * (the summation's tiles, msgb_sum_f32_tile_boxes), in a block of
+     * MSGB_TIME_TILE records taken from the pool.
+     *   slot:      (ceil(nt / MSGB_TIME_TILE), nb) block index, -1 for a dead tile;
+     *   pool:      (pool_blocks, MSGB_TIME_TILE) records in the rec32 layout;
+     *   pool_cull: (pool_blocks, 2d + 1) the culling box of each block;
+     *   pool_next: device counter of blocks taken (zeroed by the caller); a
+     *              value above pool_blocks after the call means the pool ran
+     *              out and the records are incomplete (integrate again with a
+     *              larger pool or fewer beams).
+     * Each lane of the integrator holds at most one block that no live tile
+     * took, so pool_next ends at most (live tiles + lanes). */
+    int32_t *slot;
+    void *pool;
+    float *pool_cull;
+    int64_t pool_blocks;
+    unsigned long long *pool_next;
+    const float *live_boxes;       /* (n_boxes, 2d): lo then hi of each sensor tile */
+    int64_t n_boxes;
+    double live_cutoff;
 } msgb_trajectories;
 
 enum {
@@ -256,6 +278,14 @@ int msgb_sum_fwd_f32_traj(const msgb_problem *prob, const msgb_beam_set *beams,
                           const msgb_trajectories *traj, const msgb_sum_opts *opts, int first_chunk,
                           int last_chunk, void *workspace, size_t workspace_bytes, float *out,
                           msgb_stream_t stream);
+/* Number of sensor tiles of the FP32 summation for this problem and options
+ * (opts->tiling's count, else one per 128 sensors), and their bounding boxes:
+ * boxes (n_tiles, 2 ndim) floats, lo then hi, as the summation's culling uses
+ * them.  The workspace is msgb_sum_f32_traj_workspace_size(prob, 0) bytes. */
+int64_t msgb_sum_f32_tile_count(const msgb_problem *prob, const msgb_sum_opts *opts);
+int msgb_sum_f32_tile_boxes(const msgb_problem *prob, const msgb_sum_opts *opts, void *workspace,
+                            size_t workspace_bytes, float *boxes, msgb_stream_t stream);
+
 /* g[b - b_first] for the chunk's beams (complex FP64, one entry per beam, not
  * per coefficient: the caller adds the two modes), deterministic as
  * msgb_adj_gather_f32; the workspace (sized for nb_max beams per chunk) holds

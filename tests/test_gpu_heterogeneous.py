@@ -435,3 +435,33 @@ def test_heterogeneous_3d_forward_matches_oracle_and_fp32_and_dot_test():
                          ts).cpu().numpy()
     lhs, rhs = float(np.sum(Aq * data)), float(np.sum(q * a64))
     assert abs(lhs - rhs) <= 1e-10 * abs(lhs)
+
+
+def test_compact_trajectory_store_equals_dense_records():
+    """The FP32 path's compact store (a time tile's records kept only when it
+    comes within the cutoff of a sensor tile) gives the same bits as storing
+    every record: the summation evaluates the same triples.  Also when the
+    pool runs out (a live-tile estimate far too low) and chunks are split and
+    integrated again, and when the adjoint reuses the forward's records."""
+    import beamax_b200 as bb
+
+    dev = _dev()
+    dom, wpt, p0, sens, ts, c, interp, thr = _het_case(seed=4, N=(128, 128), thr=300)
+    ode = bb.gb.gb_solvers.solve_ODE_base
+    dense = bb.MSGBSolver(thr, "top_n", 64, "spatial", ode, "scan_real", precision="fp32",
+                          compact_trajectories=False)
+    compact = bb.MSGBSolver(thr, "top_n", 64, "spatial", ode, "scan_real", precision="fp32")
+    tight = bb.MSGBSolver(thr, "top_n", 64, "spatial", ode, "scan_real", precision="fp32",
+                          trajectory_memory=4 << 20, keep_trajectories=False)
+    tight._live_est = 0.01  # far below the true fraction: the first pools overflow
+    y_d = dense.forward(p0, dom, sens, ts, wpt)
+    y_c = compact.forward(p0, dom, sens, ts, wpt)
+    y_t = tight.forward(p0, dom, sens, ts, wpt)
+    assert np.array_equal(y_d, y_c) and np.array_equal(y_d, y_t)
+    assert compact._cached_trajectories(compact.last_selection, dom, ts) is not None
+    assert 0.0 < compact._live_est < 1.0
+    data = torch.from_numpy(np.random.default_rng(2).standard_normal(y_d.shape)).to(dev).float()
+    a_d = dense.adjoint(data, dom, sens, ts, wpt)
+    a_c = compact.adjoint(data, dom, sens, ts, wpt)
+    a_t = tight.adjoint(data, dom, sens, ts, wpt)
+    assert torch.equal(a_d, a_c) and torch.equal(a_d, a_t)
