@@ -16,6 +16,8 @@
 // per save interval).  One thread per beam; the state is written at every
 // acquisition time.  A is integrated from 1 (the equation is linear in A):
 // the summation multiplies by the beam amplitude.
+#include <cstdlib>
+
 #include "traj.cuh"
 
 namespace msgb {
@@ -485,8 +487,11 @@ __device__ void launch_state(const BeamArgs &B, const TrajArgs &T, int64_t bl, S
 // i, i + stride, i + 2 stride, ... one attempted step per loop trip, so a
 // lane whose beam finishes early starts its next beam instead of idling
 // until the slowest beam of its warp is done.
-template <int D, int KIND>
-__global__ void dopri_kernel(ProbArgs P, MediumArgs med, BeamArgs B, TrajArgs T, OdeArgs o, int tt_len) {
+// MINB: resident 64-lane blocks per SM the register allocation is bounded for
+// (the stages take 43 KB of shared memory per block in 2D, so at most 5 fit).
+template <int D, int KIND, int MINB>
+__global__ void __launch_bounds__(64, MINB)
+dopri_kernel(ProbArgs P, MediumArgs med, BeamArgs B, TrajArgs T, OdeArgs o, int tt_len) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     int64_t bl = blockIdx.x * (int64_t)blockDim.x + threadIdx.x - stride;
     bool active = false;
@@ -627,24 +632,36 @@ __global__ void tr_final_kernel(ProbArgs P, MediumArgs med, TrBeamsView B, int64
 // The integrator kernels specialised for the medium kind (run-time kind ->
 // template argument).
 struct Dopri {
+    int minb;
     template <int D, int K>
-    static auto kernel() { return dopri_kernel<D, K>; }
+    auto kernel() const { return minb >= 5 ? dopri_kernel<D, K, 5> : dopri_kernel<D, K, 4>; }
 };
 struct TrFinal {
     template <int D, int K>
-    static auto kernel() { return tr_final_kernel<D, K>; }
+    auto kernel() const { return tr_final_kernel<D, K>; }
 };
+
+// Blocks per SM of the adaptive integrator: 4 (8 warps, up to 255 registers
+// per lane) unless MSGB_DOPRI_BLOCKS=5 (10 warps, registers bounded to 204).
+int dopri_blocks_per_sm() {
+    static const int v = [] {
+        const char *e = getenv("MSGB_DOPRI_BLOCKS");
+        return (e && atoi(e) == 5) ? 5 : 4;
+    }();
+    return v;
+}
+
 template <int D, typename Launch, typename Which>
-void launch_by_kind(int kind, Launch launch, Which) {
+void launch_by_kind(int kind, Launch launch, const Which &which) {
     auto go = [&](auto kern) {
         const size_t smem = dopri_smem_bytes<D>(64);
         if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         launch(kern, smem);
     };
     switch (kind) {
-        case MSGB_MEDIUM_CONSTANT: go(Which::template kernel<D, MSGB_MEDIUM_CONSTANT>()); break;
-        case MSGB_MEDIUM_LINEAR: go(Which::template kernel<D, MSGB_MEDIUM_LINEAR>()); break;
-        default: go(Which::template kernel<D, MSGB_MEDIUM_BSPLINE3>()); break;
+        case MSGB_MEDIUM_CONSTANT: go(which.template kernel<D, MSGB_MEDIUM_CONSTANT>()); break;
+        case MSGB_MEDIUM_LINEAR: go(which.template kernel<D, MSGB_MEDIUM_LINEAR>()); break;
+        default: go(which.template kernel<D, MSGB_MEDIUM_BSPLINE3>()); break;
     }
 }
 
@@ -739,15 +756,17 @@ extern "C" int msgb_ode_trajectories(const msgb_problem *prob, const msgb_medium
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        const int64_t want = 4LL * sms;
+        const int minb = dopri_blocks_per_sm();
+        const int64_t want = (int64_t)minb * sms;
         const unsigned grid = (unsigned)(need < want ? need : want);
+        const Dopri which{minb};
         switch (prob->ndim) {
             case 1: launch_by_kind<1>(M.kind, [&](auto kern, size_t sm) { kern<<<grid, blk, sm, st>>>(P, M, to_args(beams), T, O, MSGB_TIME_TILE); },
-                                      Dopri{}); break;
+                                      which); break;
             case 2: launch_by_kind<2>(M.kind, [&](auto kern, size_t sm) { kern<<<grid, blk, sm, st>>>(P, M, to_args(beams), T, O, MSGB_TIME_TILE); },
-                                      Dopri{}); break;
+                                      which); break;
             default: launch_by_kind<3>(M.kind, [&](auto kern, size_t sm) { kern<<<grid, blk, sm, st>>>(P, M, to_args(beams), T, O, MSGB_TIME_TILE); },
-                                       Dopri{}); break;
+                                       which); break;
         }
     }
     return check_launch("msgb_ode_trajectories");

@@ -469,6 +469,55 @@ def run_ode_only(args, device, peaks):
     return 0
 
 
+def run_gemm_only(args, device, peaks):
+    """The surrogate MLP's hidden-layer product alone (``--gemm-only``):
+    C16 = SiLU(A W^T + b) with A (M x 256), W (256 x 256) BF16, FP32
+    accumulation, M = args.gemm_rows, through msgb_gemm_bf16 (the TMA-fed
+    persistent tcgen05 kernel); W untimed and K timed launches, CUDA events.
+    Roofline: 2 M N K flops against the measured dense BF16 peak in
+    MEASURED_PEAKS.json when present."""
+    import torch
+
+    from beamax_b200 import _lib
+
+    torch.cuda.set_device(device)
+    M, N, K = args.gemm_rows, 256, 256
+    g = torch.Generator(device="cpu").manual_seed(0)
+    A = torch.randn(M, K, generator=g).to(torch.bfloat16).to(device)
+    W = (torch.randn(N, K, generator=g) / 16).to(torch.bfloat16).to(device)
+    b = torch.randn(N, generator=g).to(device)
+    C16 = torch.empty((M, N), dtype=torch.bfloat16, device=device)
+    err = torch.zeros(1, dtype=torch.int32, device=device)
+    gm = _lib.Gemm(A=A.data_ptr(), sAm=K, sAk=1, B=W.data_ptr(), sBn=K, sBk=1, M=M, N=N, K=K, bias=b.data_ptr(),
+                   act=1, C32=None, ldc32=0, C16=C16.data_ptr(), ldc16=N, error_flag=err.data_ptr())
+    st = torch.cuda.current_stream(device)
+    call = lambda: _lib.check(_lib.lib().msgb_gemm_bf16(_lib.ref(gm), st.cuda_stream), "msgb_gemm_bf16")
+    for _ in range(max(args.warmup, 1)):
+        call()
+    torch.cuda.synchronize(device)
+    a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    for _ in range(args.steps):
+        call()
+    e.record(st)
+    torch.cuda.synchronize(device)
+    secs = a.elapsed_time(e) / 1e3 / args.steps
+    ref = torch.nn.functional.silu(A[:4096].float() @ W.float().T + b)
+    rel = float((C16[:4096].float() - ref).norm() / ref.norm())
+    flops = 2.0 * M * N * K
+    peak_bf16 = None
+    mp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(mp):
+        with open(mp) as f:
+            peak_bf16 = json.load(f).get("bf16_tflops")
+    achieved = flops / secs / 1e12
+    hbm = (M * K * 2 + M * N * 2) / secs / 1e9
+    print(json.dumps({"mode": "gemm_only", "M": M, "N": N, "K": K, "s_per_launch": secs, "tflops": achieved,
+                      "peak_bf16_tflops": peak_bf16, "frac": achieved / peak_bf16 if peak_bf16 else None,
+                      "hbm_gbs_moved": hbm, "rel_err_vs_fp32": rel, "error_flag": int(err.item())}), flush=True)
+    return 0
+
+
 def rooflines(r, peaks, sm_mhz, args):
     """Rooflines of the step's kernels, the one with the largest device time
     per step first (``roofline``), the others after it (``roofline_other``).
@@ -605,6 +654,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-peaks", action="store_true")
     ap.add_argument("--ode-only", action="store_true", help="time the beam ODE alone (heterogeneous workloads)")
+    ap.add_argument("--gemm-only", action="store_true", help="time the surrogate's 256 x 256 layer GEMM alone")
+    ap.add_argument("--gemm-rows", type=int, default=1 << 20)
     args = ap.parse_args()
     if args.thr is None:
         args.thr = DEFAULT_THR[args.workload]
@@ -637,6 +688,8 @@ def main():
     peaks = None if args.no_peaks else measure_peaks(device)
     if args.ode_only:
         return run_ode_only(args, device, peaks)
+    if args.gemm_only:
+        return run_gemm_only(args, device, peaks)
     r = run_ours(args, rank, world, device)
     if world > 1:
         torch.distributed.destroy_process_group()
