@@ -518,6 +518,70 @@ def run_gemm_only(args, device, peaks):
     return 0
 
 
+def run_surrogate_eval(args, device, peaks):
+    """What the learned trajectory surrogate buys (``--surrogate-eval``): on
+    the workload's medium, train the MLP on ODE trajectories of a beam sample
+    (the library's own BF16 tcgen05 kernels), then time the FP32 forward with
+    and without it (CUDA events around each forward, after a warm-up of each)
+    and compare both with the FP64 forward: beams accepted, forward time, the
+    ODE time saved, rel-L2, and the MLP's inference rate."""
+    import torch
+
+    import beamax_b200 as bb
+    from beamax_b200.surrogate import TrajectorySurrogate
+
+    torch.cuda.set_device(device)
+    W = WORKLOADS[args.workload](seed=1234, thr=args.thr)
+    if not W["hetero"]:
+        raise SystemExit("--surrogate-eval needs a heterogeneous workload (het512, c3, c5)")
+    dom, wpt, sens, ts, p0 = W["domain"], W["wpt"], W["sensors"], W["ts"], W["p0"]
+    ode = bb.gb.gb_solvers.solve_ODE_base
+    s64 = bb.MSGBSolver(W["thr"], "top_n", 128, "spatial", ode, "scan_real")
+    p0_d = torch.from_numpy(p0).to(device)
+    y64 = s64.forward(p0_d, dom, sens, ts, wpt)
+    bt = s64.beams(s64.last_selection, dom, wpt)
+    t0 = time.perf_counter()
+    sur = TrajectorySurrogate(seed=0).fit(s64, dom, sens, ts, bt, n_train=args.sur_train, n_val=256, t_stride=4,
+                                          epochs=args.sur_epochs, batch=8192)
+    torch.cuda.synchronize(device)
+    t_fit = time.perf_counter() - t0
+    st = torch.cuda.current_stream(device)
+    out = {}
+    for name, kw in (("without", {}), ("with", {"surrogate": sur})):
+        s = bb.MSGBSolver(W["thr"], "top_n", 128, "spatial", ode, "scan_real", precision="fp32", **kw)
+        s.forward(p0_d, dom, sens, ts, wpt)  # warm-up
+        s.kernel_timer = []
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        y = s.forward(p0_d, dom, sens, ts, wpt)
+        b.record(st)
+        torch.cuda.synchronize(device)
+        t_ode = sum(x.elapsed_time(z) / 1e3 for nm, x, z, _ in s.kernel_timer if nm == "msgb_ode_trajectories")
+        out[name] = {"forward_s": a.elapsed_time(b) / 1e3, "ode_s": t_ode,
+                     "accepted": s.last_surrogate_accepted, "beams": 2 * bt.n,
+                     "rel_l2_vs_fp64": float(torch.linalg.norm(y64 - y.double()) / torch.linalg.norm(y64))}
+    # MLP inference rate on one chunk of feature rows
+    rows = 1 << 20
+    X = torch.zeros((rows, 16), dtype=torch.bfloat16, device=device)
+    sur._predict_rows(X)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    sur._predict_rows(X)
+    b.record(st)
+    torch.cuda.synchronize(device)
+    t_inf = a.elapsed_time(b) / 1e3
+    widths = list(sur.mlp.dims)
+    flops_row = sum(2.0 * widths[i] * widths[i + 1] for i in range(len(widths) - 1))
+    line = {"mode": "surrogate_eval", "workload": W["name"], "fit_s": t_fit, "fit_stats": sur.stats,
+            "without": out["without"], "with": out["with"],
+            "ode_s_saved": out["without"]["ode_s"] - out["with"]["ode_s"],
+            "forward_s_saved": out["without"]["forward_s"] - out["with"]["forward_s"],
+            "mlp_rows_per_s": rows / t_inf, "mlp_tflops": rows * flops_row / t_inf / 1e12,
+            "mlp_flops_per_row": flops_row}
+    print(json.dumps(line, default=float), flush=True)
+    return 0
+
+
 def rooflines(r, peaks, sm_mhz, args):
     """Rooflines of the step's kernels, the one with the largest device time
     per step first (``roofline``), the others after it (``roofline_other``).
@@ -656,6 +720,9 @@ def main():
     ap.add_argument("--ode-only", action="store_true", help="time the beam ODE alone (heterogeneous workloads)")
     ap.add_argument("--gemm-only", action="store_true", help="time the surrogate's 256 x 256 layer GEMM alone")
     ap.add_argument("--gemm-rows", type=int, default=1 << 20)
+    ap.add_argument("--surrogate-eval", action="store_true", help="train the trajectory surrogate and measure its gain")
+    ap.add_argument("--sur-train", type=int, default=3000)
+    ap.add_argument("--sur-epochs", type=int, default=40)
     args = ap.parse_args()
     if args.thr is None:
         args.thr = DEFAULT_THR[args.workload]
@@ -690,6 +757,8 @@ def main():
         return run_ode_only(args, device, peaks)
     if args.gemm_only:
         return run_gemm_only(args, device, peaks)
+    if args.surrogate_eval:
+        return run_surrogate_eval(args, device, peaks)
     r = run_ours(args, rank, world, device)
     if world > 1:
         torch.distributed.destroy_process_group()
