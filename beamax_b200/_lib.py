@@ -54,12 +54,14 @@ class MswptDesc(ctypes.Structure):
 
 class Medium(ctypes.Structure):
     _fields_ = [("kind", c_i32), ("boundary", c_i32), ("n", c_i32 * 3), ("spacing", c_dbl * 3),
-                ("origin", c_dbl * 3), ("coeffs", c_vp), ("c", c_dbl), ("lam", c_dbl)]
+                ("origin", c_dbl * 3), ("coeffs", c_vp), ("c", c_dbl), ("lam", c_dbl), ("coeffs32", c_vp),
+                ("c_ref", c_dbl)]
 
 
 class OdeOpts(ctypes.Structure):
     _fields_ = [("method", c_i32), ("substeps", c_i32), ("rtol", c_dbl), ("atol", c_dbl), ("dt0", c_dbl),
-                ("max_steps", c_i64), ("only_flagged", c_i32), ("dense_output", c_i32), ("step_count", c_vp)]
+                ("max_steps", c_i64), ("only_flagged", c_i32), ("dense_output", c_i32), ("step_count", c_vp),
+                ("medium_fp32", c_i32)]
 
 
 class SurrogateIO(ctypes.Structure):

@@ -139,10 +139,13 @@ __device__ __forceinline__ void from_full(const State<D> &f, SState<D> &s) {
 // coupled_rhs_absorption on the symmetric state (the same terms as rhs; dM
 // is formed for i <= k only).
 // (The reciprocals 1/|p| and 1/|p|^3 replace FP64 divisions.)
-template <int D, int KIND>
+template <int D, int KIND, bool F32M = false>
 __device__ void rhs_sym(const MediumArgs &med, double mode, const SState<D> &y, SState<D> &dy) {
     double c, gc[D], hc[D * D];
-    speed_eval_k<D, KIND>(med, y.x, c, gc, hc);
+    if (F32M && KIND != MSGB_MEDIUM_CONSTANT)
+        speed_eval_f32<D, KIND>(med, y.x, c, gc, hc);
+    else
+        speed_eval_k<D, KIND>(med, y.x, c, gc, hc);
     double n2 = 0.0;
 #pragma unroll
     for (int i = 0; i < D; ++i) n2 += y.p[i] * y.p[i];
@@ -316,7 +319,7 @@ constexpr size_t dopri_smem_bytes(int blk) {
     return (size_t)blk * 7 * NVS<D>::value * sizeof(double);
 }
 
-template <int D, int KIND>
+template <int D, int KIND, bool F32M = false>
 struct DopriBeam {
     SState<D> y;   // f(y) (first same as last) is stage 0 in shared memory
     double t, h, mode;
@@ -335,7 +338,7 @@ struct DopriBeam {
         rejected = false;
         code = 0;
         SState<D> f0;
-        rhs_sym<D, KIND>(med, mode, y, f0);
+        rhs_sym<D, KIND, F32M>(med, mode, y, f0);
         const double *fv = vals(f0);
 #pragma unroll
         for (int c = 0; c < NVS<D>::value; ++c) ks[c * kst] = fv[c];
@@ -387,7 +390,7 @@ struct DopriBeam {
 #pragma unroll
             for (int c = 0; c < N; ++c) tv[c] = yv[c] + hh * acc[c];
             SState<D> kn;
-            rhs_sym<D, KIND>(med, mode, yt, kn);
+            rhs_sym<D, KIND, F32M>(med, mode, yt, kn);
             const double *kv = vals(kn);
 #pragma unroll
             for (int c = 0; c < N; ++c) ks[(s * N + c) * kst] = kv[c];
@@ -489,13 +492,13 @@ __device__ void launch_state(const BeamArgs &B, const TrajArgs &T, int64_t bl, S
 // until the slowest beam of its warp is done.
 // MINB: resident 64-lane blocks per SM the register allocation is bounded for
 // (the stages take 43 KB of shared memory per block in 2D, so at most 5 fit).
-template <int D, int KIND, int MINB>
+template <int D, int KIND, int MINB, bool F32M>
 __global__ void __launch_bounds__(64, MINB)
 dopri_kernel(ProbArgs P, MediumArgs med, BeamArgs B, TrajArgs T, OdeArgs o, int tt_len) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     int64_t bl = blockIdx.x * (int64_t)blockDim.x + threadIdx.x - stride;
     bool active = false;
-    DopriBeam<D, KIND> s;
+    DopriBeam<D, KIND, F32M> s;
     s.ks = dopri_stage_smem + threadIdx.x;
     s.kst = blockDim.x;
     RecordWriter<D> rw(P, T, 0, 0.0, tt_len);
@@ -633,8 +636,12 @@ __global__ void tr_final_kernel(ProbArgs P, MediumArgs med, TrBeamsView B, int64
 // template argument).
 struct Dopri {
     int minb;
+    bool f32m;  // FP32 evaluation of the medium
     template <int D, int K>
-    auto kernel() const { return minb >= 5 ? dopri_kernel<D, K, 5> : dopri_kernel<D, K, 4>; }
+    auto kernel() const {
+        if (f32m) return minb >= 5 ? dopri_kernel<D, K, 5, true> : dopri_kernel<D, K, 4, true>;
+        return minb >= 5 ? dopri_kernel<D, K, 5, false> : dopri_kernel<D, K, 4, false>;
+    }
 };
 struct TrFinal {
     template <int D, int K>
@@ -759,7 +766,8 @@ extern "C" int msgb_ode_trajectories(const msgb_problem *prob, const msgb_medium
         const int minb = dopri_blocks_per_sm();
         const int64_t want = (int64_t)minb * sms;
         const unsigned grid = (unsigned)(need < want ? need : want);
-        const Dopri which{minb};
+        const bool f32m = opts->medium_fp32 != 0 && med->coeffs32 != nullptr && med->kind != MSGB_MEDIUM_CONSTANT;
+        const Dopri which{minb, f32m};
         switch (prob->ndim) {
             case 1: launch_by_kind<1>(M.kind, [&](auto kern, size_t sm) { kern<<<grid, blk, sm, st>>>(P, M, to_args(beams), T, O, MSGB_TIME_TILE); },
                                       which); break;

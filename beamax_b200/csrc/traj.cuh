@@ -16,6 +16,8 @@ struct MediumArgs {
     double inv_spacing[3];  // 1 / spacing (multiplications instead of FP64 divisions)
     const double *coeffs;
     double c, lam;
+    const float *coeffs32;  // (coeffs - c_ref) in FP32, or nullptr
+    double c_ref;
 };
 
 __device__ __forceinline__ int map_index(int i, int n, int boundary) {
@@ -167,6 +169,143 @@ __device__ __forceinline__ void speed_eval_k(const MediumArgs &m, const double *
 #pragma unroll
         for (int b = 0; b < D; ++b) {
             const double hv = a <= b ? hh[a][b] : hh[b][a];
+            H[a * D + b] = hv * ((a == b ? sg : sm) * m.inv_spacing[a] * m.inv_spacing[b]);
+        }
+    }
+}
+
+// The same in FP32 for the FP32 path: the fractional position is formed in
+// FP64 and rounded, the B-spline weights and tap sums run in FP32 on
+// (coefficient - c_ref) values centred on tap (1, 1[, 1]) of the stencil (the
+// weights of every derivative sum to zero, so the centring leaves the
+// gradient and Hessian unchanged and keeps their sums free of cancellation;
+// the value gets the centre back), and the results return to FP64 with c_ref.
+template <int D, int KIND>
+__device__ __forceinline__ void speed_eval_f32(const MediumArgs &m, const double *x, double &c, double *g,
+                                               double *H) {
+    constexpr bool cubic = KIND == MSGB_MEDIUM_BSPLINE3;
+    constexpr int taps = cubic ? 4 : 2;
+    constexpr int off0 = cubic ? -1 : 0;
+    constexpr int ctr = cubic ? 1 : 0;  // the tap at the cell's lower corner
+    float w[D][4], d1[D][4], d2[D][4];
+    int idx[D][4];
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        const double u = (x[a] - m.origin[a]) * m.inv_spacing[a];
+        const double fl = floor(u);
+        const float t = (float)(u - fl);
+        const int i0 = (int)fl;
+        if (cubic) {
+            const float omt = 1.0f - t, t2 = t * t, t3 = t2 * t;
+            w[a][0] = omt * omt * omt;
+            w[a][1] = fmaf(3.0f, t3, fmaf(-6.0f, t2, 4.0f));
+            w[a][2] = fmaf(-3.0f, t3, fmaf(3.0f, t2, fmaf(3.0f, t, 1.0f)));
+            w[a][3] = t3;
+            d1[a][0] = -0.5f * omt * omt;
+            d1[a][1] = fmaf(1.5f, t2, -2.0f * t);
+            d1[a][2] = fmaf(-1.5f, t2, t + 0.5f);
+            d1[a][3] = 0.5f * t2;
+            d2[a][0] = omt;
+            d2[a][1] = fmaf(3.0f, t, -2.0f);
+            d2[a][2] = fmaf(-3.0f, t, 1.0f);
+            d2[a][3] = t;
+        } else {
+            w[a][0] = 1.0f - t;
+            w[a][1] = t;
+            d1[a][0] = -1.0f;
+            d1[a][1] = 1.0f;
+            d2[a][0] = d2[a][1] = 0.0f;
+            w[a][2] = w[a][3] = d1[a][2] = d1[a][3] = d2[a][2] = d2[a][3] = 0.0f;
+        }
+#pragma unroll
+        for (int k = 0; k < taps; ++k) idx[a][k] = map_index(i0 + off0 + k, m.n[a], m.boundary);
+    }
+    float cc = 0.0f, gg[D], hh[D][D];
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+        gg[i] = 0.0f;
+#pragma unroll
+        for (int k = 0; k < D; ++k) hh[i][k] = 0.0f;
+    }
+    float vc;
+    if (D == 1) {
+        vc = __ldg(m.coeffs32 + idx[0][ctr]);
+#pragma unroll
+        for (int k = 0; k < taps; ++k) {
+            const float v = __ldg(m.coeffs32 + idx[0][k]) - vc;
+            cc = fmaf(w[0][k], v, cc);
+            gg[0] = fmaf(d1[0][k], v, gg[0]);
+            hh[0][0] = fmaf(d2[0][k], v, hh[0][0]);
+        }
+    } else if (D == 2) {
+        const int L = D - 1;
+        vc = __ldg(m.coeffs32 + (int64_t)idx[0][ctr] * m.n[L] + idx[L][ctr]);
+#pragma unroll
+        for (int i = 0; i < taps; ++i) {
+            const float *row = m.coeffs32 + (int64_t)idx[0][i] * m.n[L];
+            float rw = 0.0f, rd = 0.0f, rdd = 0.0f;
+#pragma unroll
+            for (int k = 0; k < taps; ++k) {
+                const float v = __ldg(row + idx[L][k]) - vc;
+                rw = fmaf(w[L][k], v, rw);
+                rd = fmaf(d1[L][k], v, rd);
+                rdd = fmaf(d2[L][k], v, rdd);
+            }
+            cc = fmaf(w[0][i], rw, cc);
+            gg[0] = fmaf(d1[0][i], rw, gg[0]);
+            gg[L] = fmaf(w[0][i], rd, gg[L]);
+            hh[0][0] = fmaf(d2[0][i], rw, hh[0][0]);
+            hh[0][L] = fmaf(d1[0][i], rd, hh[0][L]);
+            hh[L][L] = fmaf(w[0][i], rdd, hh[L][L]);
+        }
+    } else {
+        const int Y = 1 % D, Z = 2 % D;
+        vc = __ldg(m.coeffs32 + ((int64_t)idx[0][ctr] * m.n[Y] + idx[Y][ctr]) * m.n[Z] + idx[Z][ctr]);
+#pragma unroll
+        for (int i = 0; i < taps; ++i) {
+            float tw = 0.0f, ty = 0.0f, tyy = 0.0f, tz = 0.0f, tyz = 0.0f, tzz = 0.0f;
+#pragma unroll
+            for (int j = 0; j < taps; ++j) {
+                const float *line = m.coeffs32 + ((int64_t)idx[0][i] * m.n[Y] + idx[Y][j]) * m.n[Z];
+                float sw = 0.0f, sd = 0.0f, sdd = 0.0f;
+#pragma unroll
+                for (int k = 0; k < taps; ++k) {
+                    const float v = __ldg(line + idx[Z][k]) - vc;
+                    sw = fmaf(w[Z][k], v, sw);
+                    sd = fmaf(d1[Z][k], v, sd);
+                    sdd = fmaf(d2[Z][k], v, sdd);
+                }
+                tw = fmaf(w[Y][j], sw, tw);
+                ty = fmaf(d1[Y][j], sw, ty);
+                tyy = fmaf(d2[Y][j], sw, tyy);
+                tz = fmaf(w[Y][j], sd, tz);
+                tyz = fmaf(d1[Y][j], sd, tyz);
+                tzz = fmaf(w[Y][j], sdd, tzz);
+            }
+            cc = fmaf(w[0][i], tw, cc);
+            gg[0] = fmaf(d1[0][i], tw, gg[0]);
+            gg[Y] = fmaf(w[0][i], ty, gg[Y]);
+            gg[Z] = fmaf(w[0][i], tz, gg[Z]);
+            hh[0][0] = fmaf(d2[0][i], tw, hh[0][0]);
+            hh[0][Y] = fmaf(d1[0][i], ty, hh[0][Y]);
+            hh[0][Z] = fmaf(d1[0][i], tz, hh[0][Z]);
+            hh[Y][Y] = fmaf(w[0][i], tyy, hh[Y][Y]);
+            hh[Y][Z] = fmaf(w[0][i], tyz, hh[Y][Z]);
+            hh[Z][Z] = fmaf(w[0][i], tzz, hh[Z][Z]);
+        }
+    }
+    constexpr double s6 = cubic ? 1.0 / 6.0 : 1.0;
+    constexpr double sv = D == 1 ? s6 : (D == 2 ? s6 * s6 : s6 * s6 * s6);
+    constexpr double sg = D == 1 ? 1.0 : (D == 2 ? s6 : s6 * s6);
+    constexpr double sm = D == 3 ? s6 : 1.0;
+    // the value's weights sum to 1: the centre comes back in FP64
+    c = m.c_ref + (double)vc + (double)cc * sv;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        g[a] = (double)gg[a] * (sg * m.inv_spacing[a]);
+#pragma unroll
+        for (int b = 0; b < D; ++b) {
+            const double hv = a <= b ? (double)hh[a][b] : (double)hh[b][a];
             H[a * D + b] = hv * ((a == b ? sg : sm) * m.inv_spacing[a] * m.inv_spacing[b]);
         }
     }
@@ -436,6 +575,8 @@ inline int medium_args(const msgb_problem *prob, const msgb_medium *med, MediumA
     M.coeffs = med->coeffs;
     M.c = med->c;
     M.lam = med->lam;
+    M.coeffs32 = med->coeffs32;
+    M.c_ref = med->c_ref;
     return MSGB_OK;
 }
 

@@ -427,6 +427,15 @@ class MSGBSolver:
         coeffs = _cache.get(m, ("coeffs", str(device)), lambda: torch.from_numpy(m.coeffs).to(device))
         med.coeffs = coeffs.data_ptr()
         med.c = float(np.max(m.values))
+        if self.precision == "fp32":
+            # FP32 copy for the FP32 path's medium evaluation: offsets from the
+            # mean keep FP32's relative precision on the variation of c
+            c_ref = float(np.mean(m.coeffs))
+            c32 = _cache.get(m, ("coeffs32", str(device)),
+                             lambda: torch.from_numpy((m.coeffs - c_ref).astype(np.float32)).to(device))
+            med.coeffs32 = c32.data_ptr()
+            med.c_ref = c_ref
+            return med, (coeffs, c32)
         return med, coeffs
 
     @staticmethod
@@ -453,7 +462,8 @@ class MSGBSolver:
             return _lib.OdeOpts(method=0, substeps=self.rk4_substeps)
         return _lib.OdeOpts(method=1, substeps=1, rtol=float(cfg.rtol), atol=float(cfg.atol),
                             dt0=float(cfg.dt0) if cfg.dt0 is not None else 0.0, max_steps=int(cfg.max_steps),
-                            dense_output=int(bool(cfg.dense_output)))
+                            dense_output=int(bool(cfg.dense_output)),
+                            medium_fp32=int(self.precision == "fp32"))
 
     def _mode_chunks(self, domain: Domain, nt: int, bt: BeamTensors, fp64: bool):
         """Chunks over the beams of the summed branches: [0, 2n), [0, n) (mode

@@ -180,6 +180,8 @@ typedef struct msgb_medium {
     const double *coeffs;    /* device, prod(n) values (C order) */
     double c;                /* kind CONSTANT */
     double lam;              /* absorption lambda of coupled_rhs_absorption */
+    const float *coeffs32;   /* optional: (coeffs - c_ref) in FP32, for msgb_ode_opts.medium_fp32 */
+    double c_ref;
 } msgb_medium;
 
 /* Trajectory output for beams [b_first, b_first + nb) of the 2n beams (b >= n:
@@ -247,6 +249,10 @@ typedef struct msgb_ode_opts {
                                 control and save times come from the continuous extension */
     unsigned long long *step_count; /* optional device counter (NULL: none): attempted
                                 DOPRI5 steps (accepted + rejected) of the call are added to it */
+    int32_t medium_fp32;     /* DOPRI5 with a grid medium and med->coeffs32: evaluate c, grad c
+                                and hess c in FP32 (taps centred on the nearest one, result
+                                + c_ref in FP64); the ray, Riccati and amplitude stay FP64.
+                                For the FP32 path; the FP64 path evaluates in FP64. */
 } msgb_ode_opts;
 
 /* FP64 integration of coupled_rhs_absorption (gb/gb_solvers.py:787-867) for
