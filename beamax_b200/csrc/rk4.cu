@@ -319,7 +319,10 @@ constexpr size_t dopri_smem_bytes(int blk) {
     return (size_t)blk * 7 * NVS<D>::value * sizeof(double);
 }
 
-template <int D, int KIND, bool F32M = false>
+// DENSE: save times may fall inside a step (msgb_ode_opts.dense_output);
+// without it every step ends on a save time and the continuous extension is
+// not compiled (it is what pushed the kernel past 255 registers).
+template <int D, int KIND, bool F32M = false, bool DENSE = true>
 struct DopriBeam {
     SState<D> y;   // f(y) (first same as last) is stage 0 in shared memory
     double t, h, mode;
@@ -428,7 +431,7 @@ struct DopriBeam {
             rejected = false;
             const double t_new = last ? target : t + hh;
             while (k < P.nt && P.ts[k] <= t_new) {
-                if (P.ts[k] == t_new) {
+                if (!DENSE || P.ts[k] == t_new) {
                     State<D> yf;
                     to_full(yt, yf);
                     rw.put(k, yf, false);
@@ -492,13 +495,13 @@ __device__ void launch_state(const BeamArgs &B, const TrajArgs &T, int64_t bl, S
 // until the slowest beam of its warp is done.
 // MINB: resident 64-lane blocks per SM the register allocation is bounded for
 // (the stages take 43 KB of shared memory per block in 2D, so at most 5 fit).
-template <int D, int KIND, int MINB, bool F32M>
+template <int D, int KIND, int MINB, bool F32M, bool DENSE>
 __global__ void __launch_bounds__(64, MINB)
 dopri_kernel(ProbArgs P, MediumArgs med, BeamArgs B, TrajArgs T, OdeArgs o, int tt_len) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     int64_t bl = blockIdx.x * (int64_t)blockDim.x + threadIdx.x - stride;
     bool active = false;
-    DopriBeam<D, KIND, F32M> s;
+    DopriBeam<D, KIND, F32M, DENSE> s;
     s.ks = dopri_stage_smem + threadIdx.x;
     s.kst = blockDim.x;
     RecordWriter<D> rw(P, T, 0, 0.0, tt_len);
@@ -636,11 +639,13 @@ __global__ void tr_final_kernel(ProbArgs P, MediumArgs med, TrBeamsView B, int64
 // template argument).
 struct Dopri {
     int minb;
-    bool f32m;  // FP32 evaluation of the medium
+    bool f32m;   // FP32 evaluation of the medium
+    bool dense;  // save times from the continuous extension
     template <int D, int K>
     auto kernel() const {
-        if (f32m) return minb >= 5 ? dopri_kernel<D, K, 5, true> : dopri_kernel<D, K, 4, true>;
-        return minb >= 5 ? dopri_kernel<D, K, 5, false> : dopri_kernel<D, K, 4, false>;
+        if (dense) return f32m ? dopri_kernel<D, K, 4, true, true> : dopri_kernel<D, K, 4, false, true>;
+        if (f32m) return minb >= 5 ? dopri_kernel<D, K, 5, true, false> : dopri_kernel<D, K, 4, true, false>;
+        return minb >= 5 ? dopri_kernel<D, K, 5, false, false> : dopri_kernel<D, K, 4, false, false>;
     }
 };
 struct TrFinal {
@@ -767,7 +772,7 @@ extern "C" int msgb_ode_trajectories(const msgb_problem *prob, const msgb_medium
         const int64_t want = (int64_t)minb * sms;
         const unsigned grid = (unsigned)(need < want ? need : want);
         const bool f32m = opts->medium_fp32 != 0 && med->coeffs32 != nullptr && med->kind != MSGB_MEDIUM_CONSTANT;
-        const Dopri which{minb, f32m};
+        const Dopri which{minb, f32m, opts->dense_output != 0};
         switch (prob->ndim) {
             case 1: launch_by_kind<1>(M.kind, [&](auto kern, size_t sm) { kern<<<grid, blk, sm, st>>>(P, M, to_args(beams), T, O, MSGB_TIME_TILE); },
                                       which); break;

@@ -208,6 +208,8 @@ class MSGBSolver:
         self._traj_owner = None
         self._live_est = 0.5  # fraction of (time tile, beam) pairs the compact store keeps
         self._compact_kept = None
+        # (b_first, nb, pool blocks, blocks taken) of every compact integration
+        self.compact_log = []
         # When set to a list, every FP32 summation entry point call appends
         # (name, start event, end event, evaluation counter) recorded on the
         # launching stream around the call.
@@ -607,6 +609,7 @@ class MSGBSolver:
                                                             _lib.ref(opts_ode), _lib.ref(tr), st),
                            "msgb_ode_trajectories")
             used = int(ctr.item())
+            self.compact_log.append((b_first, nb, blocks, used))
             if used > blocks:
                 if nb == 1:
                     raise RuntimeError("compact trajectory store: one beam needs more than the budget")
@@ -687,10 +690,12 @@ class MSGBSolver:
             lo, hi = chunks[0][0], chunks[-1][0] + chunks[-1][1]
             keep = self.keep_trajectories and self._traj_owner is not None
             self._compact_kept = None
+            # the forward keeps its Kahan state in this workspace from the first
+            # chunk to the last: one size (no per-chunk partials), never regrown
+            nbytes = _lib.lib().msgb_sum_f32_traj_workspace_size(_lib.ref(pr), 0)
+            ws = workspace(dev, "sum32traj", nbytes)
             for tr, first, last in self._compact_integrate(pr, med, bs, lo, hi, domain, sensors, opts, dev, st,
                                                           status, keep=keep):
-                nbytes = _lib.lib().msgb_sum_f32_traj_workspace_size(_lib.ref(pr), tr.nb)
-                ws = workspace(dev, "sum32traj", nbytes)
                 with self._kernel_span("msgb_sum_fwd_f32_traj", cnt):
                     _lib.check(_lib.lib().msgb_sum_fwd_f32_traj(_lib.ref(pr), _lib.ref(bs), _lib.ref(tr),
                                                                 _lib.ref(opts), int(first), int(last), ws.data_ptr(),
