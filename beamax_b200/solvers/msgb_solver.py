@@ -533,10 +533,13 @@ class MSGBSolver:
 
     def _trajectory_budget(self, dev) -> int:
         """Bytes for one chunk of trajectory records: trajectory_memory, or
-        what the device has free less 4 GiB of headroom."""
+        what the device has free less 4 GiB of headroom.  Free includes the
+        memory torch's allocator holds in its cache (freed tensors, e.g. the
+        previous step's records), which it hands out again."""
         import torch
 
         free, _ = torch.cuda.mem_get_info(dev)
+        free += torch.cuda.memory_reserved(dev) - torch.cuda.memory_allocated(dev)
         return int(max(1 << 20, min(self.trajectory_memory, free - (4 << 30))))
 
     def _compact_chunk_beams(self, d, nt, nbeam, budget):
@@ -731,8 +734,7 @@ class MSGBSolver:
             return None
         self._traj_cache = None  # free the previous forward's records first
         size = per * chunks[-1][1] + 4096
-        free, _ = torch.cuda.mem_get_info(dev)
-        if free < size + (4 << 30):
+        if self._trajectory_budget(dev) < size:
             return None
         return torch.empty(size, dtype=torch.uint8, device=dev)
 
