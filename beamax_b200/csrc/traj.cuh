@@ -453,7 +453,7 @@ struct RecordWriter {
         char *rec32_base = nullptr;
         if (T.pool) {
             if (kk_tile == 0 && blk < 0) blk = (int64_t)atomicAdd(T.pool_next, 1ULL);
-            if (blk < T.pool_blocks)
+            if (blk >= 0 && blk < T.pool_blocks)
                 rec32_base = (char *)T.pool + (blk * tt_len + kk_tile) * (int64_t)(16 * D + 8 * S + 8);
         } else if (T.rec32) {
             rec32_base = (char *)T.rec32 + (k * T.nb + bl) * (int64_t)(16 * D + 8 * S + 8);

@@ -472,7 +472,10 @@ class MSGBSolver:
         +1 only) or [n, 2n) (mode -1 only)."""
         n = bt.n
         lo, hi = {0: (0, 2 * n), 1: (0, n), 2: (n, 2 * n)}[bt.modes]
-        chunks, per, n_tt = self._chunks(domain, nt, hi - lo, fp64, self._trajectory_budget(bt.x0.device))
+        budget = self._trajectory_budget(bt.x0.device)
+        if self.keep_trajectories and (fp64 or not self._compact()):
+            budget //= 2  # the dense path may hold a kept chunk beside the chunk buffer
+        chunks, per, n_tt = self._chunks(domain, nt, hi - lo, fp64, budget)
         return [(lo + b, nb) for b, nb in chunks], per, n_tt
 
     def _trajectories(self, pr, med, bs, b_first, nb, fp64, per, n_tt, dev, st, status, buf=None):
@@ -737,6 +740,11 @@ class MSGBSolver:
         if self._trajectory_budget(dev) < size:
             return None
         return torch.empty(size, dtype=torch.uint8, device=dev)
+
+    def release_trajectories(self) -> None:
+        """Drop the trajectory records kept for the next adjoint (frees their
+        device memory)."""
+        self._traj_cache = None
 
     def _propagation_key(self, domain):
         """What the kept records depend on besides the selection and the time

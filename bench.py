@@ -389,6 +389,7 @@ def run_ours(args, rank, world, device):
               "levels": wpt.dyadic_decomp.num_levels, "workload": W["name"]}
 
     # FP64 plain path (dense, reference semantics): once, also the accuracy reference
+    s32.release_trajectories()
     if rank == 0 and not args.no_fp64:
         flush.zero_()
         torch.cuda.synchronize()
