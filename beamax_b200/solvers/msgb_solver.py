@@ -601,7 +601,24 @@ class MSGBSolver:
         widest = max(nb for _, nb in todo)
         need = int(widest * n_tt * (4 + self._live_est * (block + cull)) + min(widest, lanes) * (block + cull)
                    + 4096)
-        buf = torch.empty(min(budget, need), dtype=torch.uint8, device=dev)
+        buf = None
+        size = min(budget, need)
+        while buf is None:
+            try:
+                buf = torch.empty(size, dtype=torch.uint8, device=dev)
+            except torch.OutOfMemoryError:
+                # the allocator's cache may be fragmented: return it to the
+                # driver and retry once at this size, then halve the chunks
+                torch.cuda.empty_cache()
+                try:
+                    buf = torch.empty(size, dtype=torch.uint8, device=dev)
+                except torch.OutOfMemoryError:
+                    if widest == 1:
+                        raise
+                    widest = (widest + 1) // 2
+                    todo = [(x, min(widest, b0 + n0 - x)) for b0, n0 in todo for x in range(b0, b0 + n0, widest)]
+                    size = int(widest * n_tt * (4 + self._live_est * (block + cull))
+                               + min(widest, lanes) * (block + cull) + 4096)
         first = True
         opts_ode = self._ode_opts(None)
         if self.ode_step_counter is not None:
