@@ -1060,6 +1060,7 @@ struct Layout {
         total;
     size_t cub_bytes;
     int64_t n_st;
+    int64_t cull_cap;  // beams the culling table has room for
 };
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
@@ -1091,7 +1092,8 @@ Layout layout(const msgb_problem *p, int64_t n_beams, bool with_data, int64_t n_
     l.hn = o; o = align256(o + ns * D * 4);
     l.seed = o; o = align256(o + ns + 1);
     l.sorted = o; o = align256(o + ns * D * 8);
-    l.cull = o; o = align256(o + (n_beams > 0 ? n_beams : 1) * sizeof(Cull<3>));
+    l.cull_cap = n_beams > 0 ? n_beams : 1;
+    l.cull = o; o = align256(o + l.cull_cap * sizeof(Cull<3>));
     l.data = o; o = align256(o + (with_data ? p->nt * ns * 4 : 0));
     l.work = o; o = align256(o + 64);
     // adjoint partials: one complex FP64 per (time tile, beam mode) of the coefficients
@@ -1141,6 +1143,8 @@ template <int D>
 int prep(const msgb_problem *p, const msgb_beam_set *b, const msgb_sum_opts *o, const Layout &l, char *ws,
          cudaStream_t st) {
     const int64_t ns = p->ns;
+    if (b->n > l.cull_cap) return fail(MSGB_ERR_WORKSPACE, "culling table sized for %lld beams, got %lld",
+                                       (long long)l.cull_cap, (long long)b->n);
     uint32_t *kin = (uint32_t *)(ws + l.keys_in), *kout = (uint32_t *)(ws + l.keys_out);
     int32_t *vin = (int32_t *)(ws + l.vals_in), *vout = (int32_t *)(ws + l.vals_out);
     int32_t *offs = (int32_t *)(ws + l.offs);
@@ -1177,7 +1181,10 @@ int sm_count() {
 template <int D, bool TRAJ>
 int run_fwd(const msgb_problem *p, const msgb_beam_set *b, const msgb_sum_opts *o, char *ws, const Layout &l,
             float *out, cudaStream_t st, TrajSrc<D> T) {
-    if (int e = prep<D>(p, b, o, l, ws, st)) return e;
+    // trajectory sums cull with the records' own boxes: the closed-form
+    // culling table (sized for no beams in their layout) is not built
+    msgb_beam_set none{};
+    if (int e = prep<D>(p, TRAJ ? &none : b, o, l, ws, st)) return e;
     const int64_t n_st = l.n_st, n_tt = (p->nt + TT - 1) / TT;
     if (n_st * n_tt > 0x7fffffffLL) return fail(MSGB_ERR_UNSUPPORTED, "msgb_sum_fwd_f32: too many tiles");
     ProbArgs P = to_args(p);
@@ -1207,7 +1214,8 @@ int run_fwd(const msgb_problem *p, const msgb_beam_set *b, const msgb_sum_opts *
 template <int D, bool TRAJ>
 int run_adj(const msgb_problem *p, const msgb_beam_set *b, const msgb_sum_opts *o, char *ws, const Layout &l,
             const float *data, double *part, double *g, cudaStream_t st, TrajSrc<D> T) {
-    if (int e = prep<D>(p, b, o, l, ws, st)) return e;
+    msgb_beam_set none{};
+    if (int e = prep<D>(p, TRAJ ? &none : b, o, l, ws, st)) return e;
     dim3 tg((unsigned)((p->ns + 31) / 32), (unsigned)((p->nt + 31) / 32));
     if (tg.y > 65535u) return fail(MSGB_ERR_UNSUPPORTED, "msgb_adj_gather_f32: nt too large");
     transpose_permute_kernel<<<tg, dim3(32, 8), 0, st>>>(data, (const int32_t *)(ws + l.vals_out), p->nt, p->ns,

@@ -273,6 +273,7 @@ class MSGBSolver:
         pr.ts = ts_d.data_ptr()
         pr.ns = pos.shape[0]
         pr.sensors = sd.data_ptr()
+        pr._owned = (ts_d, sd)  # the device arrays live as long as the struct that points at them
         return pr, (ts_d, sd)
 
     def _tiling(self, domain: Domain, sensors, device):
@@ -711,14 +712,14 @@ class MSGBSolver:
         if self._compact():
             keep_buf = None  # the compact path keeps its own last chunk
             lo, hi = chunks[0][0], chunks[-1][0] + chunks[-1][1]
-            keep = self.keep_trajectories and self._traj_owner is not None
+            keep_last = self.keep_trajectories and self._traj_owner is not None
             self._compact_kept = None
             # the forward keeps its Kahan state in this workspace from the first
             # chunk to the last: one size (no per-chunk partials), never regrown
             nbytes = _lib.lib().msgb_sum_f32_traj_workspace_size(_lib.ref(pr), 0)
             ws = workspace(dev, "sum32traj", nbytes)
             for tr, first, last in self._compact_integrate(pr, med, bs, lo, hi, domain, sensors, opts, dev, st,
-                                                          status, keep=keep):
+                                                          status, keep=keep_last):
                 with self._kernel_span("msgb_sum_fwd_f32_traj", cnt):
                     _lib.check(_lib.lib().msgb_sum_fwd_f32_traj(_lib.ref(pr), _lib.ref(bs), _lib.ref(tr),
                                                                 _lib.ref(opts), int(first), int(last), ws.data_ptr(),

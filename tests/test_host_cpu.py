@@ -303,3 +303,25 @@ def test_threshold_configuration_is_validated(threshold, strategy, match):
     """tests/solvers/test_msgb_solver_misc.py:424-446."""
     with pytest.raises(ValueError, match=match):
         bb.MSGBSolver(threshold, strategy, 4, "spatial", bb.gb.gb_solvers.solve_ODE_base, "all_real")
+
+
+def test_problem_struct_owns_its_device_arrays():
+    """The problem struct keeps the time and sensor arrays it points at alive,
+    whatever the caller does with the second return value (a rebound name
+    once let the allocator hand the time array to another tensor while the
+    kernels still read it)."""
+    import gc
+
+    pytest.importorskip("torch")
+    dom = bb.Domain(N=(32, 32), dx=(1e-4, 1e-4), c=1500.0, cfl=0.3, periodic=(False, False))
+    mask = np.zeros((32, 32))
+    mask[0, :] = 1
+    sens = bb.Sensor(dom, binary_mask=mask)
+    ts = dom.generate_time_domain()[:10]
+    s = bb.MSGBSolver(64, "top_n", 16, "spatial", bb.gb.gb_solvers.solve_hom_diag, "scan_real")
+    pr, held = s._problem(dom, sens, ts, "cpu")
+    ptr = held[0].data_ptr()
+    del held
+    gc.collect()
+    assert pr.ts == ptr and pr._owned[0].data_ptr() == ptr
+    assert np.array_equal(pr._owned[0].numpy(), np.asarray(ts, np.float64))
