@@ -25,6 +25,7 @@ reversal (:984-1111), both from boundary data with ``msgb_tr_init`` and
 
 from __future__ import annotations
 
+import collections
 import contextlib
 import ctypes
 import math
@@ -208,8 +209,8 @@ class MSGBSolver:
         self._traj_owner = None
         self._live_est = 0.5  # fraction of (time tile, beam) pairs the compact store keeps
         self._compact_kept = None
-        # (b_first, nb, pool blocks, blocks taken) of every compact integration
-        self.compact_log = []
+        # (b_first, nb, pool blocks, blocks taken) of the last 256 compact integrations
+        self.compact_log = collections.deque(maxlen=256)
         # When set to a list, every FP32 summation entry point call appends
         # (name, start event, end event, evaluation counter) recorded on the
         # launching stream around the call.
