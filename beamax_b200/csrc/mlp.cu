@@ -377,6 +377,8 @@ gemm_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         }
     } else {
         const int quarter = warp & 3;  // TMEM lanes 32 quarter .. + 31
+        const bool vec32 = g.C32 && (g.ldc32 & 3) == 0 && ((uintptr_t)g.C32 & 15) == 0;
+        const bool vec16 = g.C16 && (g.ldc16 & 7) == 0 && ((uintptr_t)g.C16 & 15) == 0;
         bool ok = true;
         for (int it = 0; it < n_local && ok; ++it) {
             const int a = it & 1, use = it >> 1;
@@ -399,12 +401,43 @@ gemm_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                     : "r"(taddr));
                 asm volatile("tcgen05.wait::ld.sync.aligned;");
                 if (row < g.M) {
+                    float z[16];
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) {
-                        const int col = col0 + j;
-                        float z = __uint_as_float(r[j]) + (g.bias ? g.bias[col] : 0.0f);
-                        if (g.C32) g.C32[row * g.ldc32 + col] = z;
-                        if (g.C16) g.C16[row * g.ldc16 + col] = __float2bfloat16(g.act == 1 ? silu(z) : z);
+                    for (int j = 0; j < 16; ++j) z[j] = __uint_as_float(r[j]) + (g.bias ? g.bias[col0 + j] : 0.0f);
+                    // a lane's 16 columns are contiguous in its row: 16-byte stores
+                    // where the output's base and row stride allow them
+                    if (g.C32) {
+                        float *dst = g.C32 + row * g.ldc32 + col0;
+                        if (vec32) {
+#pragma unroll
+                            for (int j = 0; j < 16; j += 4)
+                                *reinterpret_cast<float4 *>(dst + j) = make_float4(z[j], z[j + 1], z[j + 2], z[j + 3]);
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < 16; ++j) dst[j] = z[j];
+                        }
+                    }
+                    if (g.C16) {
+                        uint32_t h[8];
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            const float u = g.act == 1 ? silu(z[2 * j]) : z[2 * j];
+                            const float v = g.act == 1 ? silu(z[2 * j + 1]) : z[2 * j + 1];
+                            const __nv_bfloat162 b2 = __floats2bfloat162_rn(u, v);  // .x = u (lower address)
+                            h[j] = *reinterpret_cast<const uint32_t *>(&b2);
+                        }
+                        __nv_bfloat16 *dst = g.C16 + row * g.ldc16 + col0;
+                        if (vec16) {
+                            reinterpret_cast<uint4 *>(dst)[0] = make_uint4(h[0], h[1], h[2], h[3]);
+                            reinterpret_cast<uint4 *>(dst)[1] = make_uint4(h[4], h[5], h[6], h[7]);
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < 8; ++j) {
+                                const __nv_bfloat162 b2 = *reinterpret_cast<const __nv_bfloat162 *>(&h[j]);
+                                dst[2 * j] = b2.x;
+                                dst[2 * j + 1] = b2.y;
+                            }
+                        }
                     }
                 }
             }

@@ -443,10 +443,9 @@ def test_compact_trajectory_store_equals_dense_records():
     every record when both hold all beams in one chunk: the summation
     evaluates the same triples in the same order.  When the pool runs out (a
     live-tile estimate far too low) and chunks are split and integrated
-    again, the forward pairs other beams in its paired FP32 sums (1e-6
-    rel-L2) while the transpose, whose per-beam sums do not depend on the
-    pairing, keeps the same bits; also when the adjoint reuses the forward's
-    records."""
+    again, both directions pair other beams in their paired FP32 sums (a
+    pair whose partner needs the direct evaluation is evaluated directly):
+    1e-6 rel-L2.  Also when the adjoint reuses the forward's records."""
     import beamax_b200 as bb
 
     dev = _dev()
@@ -471,4 +470,6 @@ def test_compact_trajectory_store_equals_dense_records():
     a_d = dense.adjoint(data, dom, sens, ts, wpt)
     a_c = compact.adjoint(data, dom, sens, ts, wpt)
     a_t = tight.adjoint(data, dom, sens, ts, wpt)
-    assert torch.equal(a_d, a_c) and torch.equal(a_d, a_t)
+    assert torch.equal(a_d, a_c)
+    rel = float(torch.linalg.vector_norm(a_t - a_d) / torch.linalg.vector_norm(a_d))
+    assert rel <= 1e-6, rel
