@@ -362,74 +362,6 @@ __device__ __forceinline__ bool survives(const Cull<D> &cb, float c0, float ta, 
     return 0.5f * cb.w * lam * d2 * 0.999f <= cutoff;
 }
 
-// The cut of one (beam, time tile) as 2D + 1 floats: the bounding box of the
-// beam centre's path over the time tile (open on periodic axes) and k with
-// chi >= k dist^2 (0 when the beam is never cut).  cut_near() against a box
-// is then survives() / traj_survives() with that box: the per-warp test
-// against the warp's own group of GS sensors.
-template <int D>
-__device__ __forceinline__ void closed_cut(const Cull<D> &cb, float c0, float ta, float tb, const ProbArgs &P,
-                                           float cutoff, float *box) {
-    const bool open = !cb.ok || cutoff <= 0.0f;
-#pragma unroll
-    for (int i = 0; i < D; ++i) {
-        if (open || P.periodic[i]) {
-            box[i] = -3.4e38f;
-            box[D + i] = 3.4e38f;
-            continue;
-        }
-        const float v = c0 * cb.dir[i];
-        const float xa = fmaf(v, ta, cb.x0[i]), xb = fmaf(v, tb, cb.x0[i]);
-        box[i] = fminf(xa, xb);
-        box[D + i] = fmaxf(xa, xb);
-    }
-    if (open) {
-        box[2 * D] = 0.0f;
-        return;
-    }
-    const float k = fabsf(c0) * fmaxf(fabsf(ta), fabsf(tb)) * cb.inv_np;
-    const float lam = 1.0f / (1.0f / cb.bmin + k * k * cb.bmax);
-    box[2 * D] = 0.5f * cb.w * lam;
-}
-
-template <int D>
-__device__ __forceinline__ bool cut_near(const float *box, const TileInfo<D> &g, float cutoff) {
-    if (cutoff <= 0.0f) return true;
-    float d2 = 0.0f;
-#pragma unroll
-    for (int i = 0; i < D; ++i) {
-        const float gap = fmaxf(0.0f, fmaxf(g.lo[i] - box[D + i], box[i] - g.hi[i]));
-        d2 = fmaf(gap, gap, d2);
-    }
-    return box[2 * D] * d2 * 0.999f <= cutoff;
-}
-
-// Bounding box of this warp's group of GS sensors (sensors gbase ... of the
-// tile; ds_g holds their FP32 offsets from the tile centre s0).  Every lane
-// of the warp calls it.
-template <int D>
-__device__ __forceinline__ TileInfo<D> group_box(const float *ds_g, int64_t s_first, int gbase, int s_cnt,
-                                                 const TileInfo<D> &ti, int lane) {
-    TileInfo<D> g = ti;
-    const int k = gbase + (lane & (GS - 1));
-    const bool ok = k < s_cnt;
-#pragma unroll
-    for (int i = 0; i < D; ++i) {
-        const float v = ok ? ds_g[(s_first + k) * D + i] : 0.0f;
-        float lo = ok ? v : 3.4e38f, hi = ok ? v : -3.4e38f;
-#pragma unroll
-        for (int o = GS / 2; o > 0; o >>= 1) {
-            lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-            hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-        }
-        if (lo <= hi) {
-            g.lo[i] = (float)(ti.s0[i] + (double)lo);
-            g.hi[i] = (float)(ti.s0[i] + (double)hi);
-        }
-    }
-    return g;
-}
-
 // ------------------------------------------------------------------ prep
 // Sort key: Morton order of coarse cells (32 per axis), row-major inside a
 // cell, so axis-aligned lines and planes form evenly spaced runs.
@@ -615,21 +547,6 @@ __device__ __forceinline__ bool traj_survives(const TrajSrc<D> &T, int64_t bl, i
     return c[2 * D] * d2 * 0.999f <= cutoff;
 }
 
-// The record's culling box of a surviving (beam, time tile) in cut form.
-template <int D>
-__device__ __forceinline__ void traj_cut(const TrajSrc<D> &T, int64_t bl, int64_t tt, float cutoff, float *box) {
-    if (cutoff <= 0.0f) {
-#pragma unroll
-        for (int i = 0; i < D; ++i) box[i] = -3.4e38f, box[D + i] = 3.4e38f;
-        box[2 * D] = 0.0f;
-        return;
-    }
-    const float *c = T.pool ? T.pool_cull + (int64_t)T.slot[tt * T.nb + bl] * (2 * D + 1)
-                            : T.cull + (tt * T.nb + bl) * (2 * D + 1);
-#pragma unroll
-    for (int i = 0; i < 2 * D + 1; ++i) box[i] = c[i];
-}
-
 template <int D>
 __device__ __forceinline__ void traj_beam_time(const BeamArgs &B, const TrajSrc<D> &T, int64_t bl, int64_t k,
                                                BeamTime<D> &bt) {
@@ -670,7 +587,6 @@ fwd32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
              int n_tiles, TrajSrc<D> T) {
     constexpr int NF = Rec<D>::NF;
     __shared__ float rec[NF][G][TT];
-    __shared__ float sbox[G][2 * D + 1];  // the pass's beams in cut form
     __shared__ float sds[TS][D], shn[TS][D];
     __shared__ uint8_t sseed[TS + 1];
     __shared__ int64_t surv[2 * THREADS];
@@ -702,8 +618,6 @@ fwd32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
         const bool fast = gfast_g[st * NW + warp] != 0;
         const int gbase = warp * GS;
         const bool active = gbase < s_cnt;
-        const TileInfo<D> gi = group_box<D>(ds_g, s_first, gbase, s_cnt, ti, lane);
-        const unsigned long long g_evals = (unsigned long long)t_cnt * (unsigned long long)max(0, min(GS, s_cnt - gbase));
         // Kahan sums of sensors 2h and 2h + 1 in .x and .y
         float2 acc2[GS / 2], cmp2[GS / 2];
 #pragma unroll
@@ -753,19 +667,10 @@ fwd32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
             if (tid == 0) nsurv_s = tot;
             __syncthreads();
             const int nsurv = nsurv_s;
+            evals += (unsigned long long)nsurv * (unsigned long long)t_cnt * (unsigned long long)s_cnt;
             for (int g0 = 0; g0 < nsurv; g0 += G) {
                 {
                     const int gl = tid / TT, tloc = tid % TT;
-                    if (tloc == 0 && g0 + gl < nsurv) {
-                        const int64_t sj = surv[g0 + gl];
-                        if (TRAJ) {
-                            traj_cut<D>(T, sj, tt, cutoff, sbox[gl]);
-                        } else {
-                            const bool mi = sj >= B.n;
-                            closed_cut<D>(cull[mi ? sj - B.n : sj], mi ? -(float)P.c : (float)P.c, ta, tb, P, cutoff,
-                                          sbox[gl]);
-                        }
-                    }
                     Rec<D> r;
                     if (g0 + gl < nsurv && tloc < t_cnt) {
                         BeamTime<D> bt;
@@ -790,27 +695,14 @@ fwd32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
                 const int ng = min(G, nsurv - g0);
                 if (active) {
                     for (int gl = 0; gl < ng; gl += 2) {
-                        // the pair against this warp's group (warp-uniform)
-                        const bool ua = cut_near<D>(sbox[gl], gi, cutoff);
-                        const bool ub = gl + 1 < ng && cut_near<D>(sbox[gl + 1], gi, cutoff);
-                        if (!ua && !ub) continue;
-                        if (lane == 0) evals += (unsigned long long)(ua + ub) * g_evals;
                         Rec<D> ra, rb;
                         load_rec<D>(rec, gl, lane, ra);
                         load_rec<D>(rec, gl + 1, lane, rb);  // zero-amplitude record when gl + 1 == ng
-                        if (!ua) ra.amp = 0.0f;
-                        if (!ub) rb.amp = 0.0f;
                         cf za, fa, qa, zb, fb, qb;
                         int ka = kRunRecurrence, kb = kRunRecurrence;
                         if (fast) {
-                            if (ua)
-                                za = seed_eval<D, false>(ra, sds[gbase], shn[gbase], true, P, fa, qa, &ka, cutoff > 0.0f);
-                            else
-                                ka = kRunNegligible;
-                            if (ub)
-                                zb = seed_eval<D, false>(rb, sds[gbase], shn[gbase], true, P, fb, qb, &kb, cutoff > 0.0f);
-                            else
-                                kb = kRunNegligible;
+                            za = seed_eval<D, false>(ra, sds[gbase], shn[gbase], true, P, fa, qa, &ka, cutoff > 0.0f);
+                            zb = seed_eval<D, false>(rb, sds[gbase], shn[gbase], true, P, fb, qb, &kb, cutoff > 0.0f);
                             if (ka == kRunNegligible) za = fa = qa = cf{0.0f, 0.0f};
                             if (kb == kRunNegligible) zb = fb = qb = cf{0.0f, 0.0f};
                         }
@@ -893,7 +785,7 @@ fwd32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
         }
         __syncthreads();
     }
-    if (eval_count && lane == 0 && evals) atomicAdd(eval_count, evals);  // per warp: its group's evaluations
+    if (eval_count && tid == 0 && evals) atomicAdd(eval_count, evals);
 }
 
 // ------------------------------------------------------------------ adjoint
@@ -930,7 +822,6 @@ adj32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
     constexpr int NF = Rec<D>::NF;
     constexpr int RJ = AdjRange<TRAJ>::RJ;
     __shared__ float rec[NF][G][TT];
-    __shared__ float sbox[G][2 * D + 1];  // the pass's beams in cut form
     __shared__ float sds[TS][D], shn[TS][D];
     __shared__ int32_t surv[2 * THREADS];
     __shared__ int warp_cnt[NW];
@@ -970,9 +861,6 @@ adj32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
             const bool fast = gfast_g[st * NW + warp] != 0;
             const int gbase = warp * GS;
             const bool active = gbase < s_cnt;
-            const TileInfo<D> gi = group_box<D>(ds_g, s_first, gbase, s_cnt, ti, lane);
-            const unsigned long long g_evals =
-                (unsigned long long)t_cnt * (unsigned long long)max(0, min(GS, s_cnt - gbase));
             const float *dcol = dataT + (int64_t)s_first * P.nt + t_first + lane;
             float dv[GS];
 #pragma unroll
@@ -1008,17 +896,10 @@ adj32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
                 if (tid == 0) nsurv_s = tot;
                 __syncthreads();
                 const int nsurv = nsurv_s;
+                evals += (unsigned long long)nsurv * (unsigned long long)t_cnt * (unsigned long long)s_cnt;
                 for (int g0 = 0; g0 < nsurv; g0 += G) {
                     {
                         const int gl = tid / TT, tloc = tid % TT;
-                        if (tloc == 0 && g0 + gl < nsurv) {
-                            const int q = surv[g0 + gl];
-                            if (TRAJ)
-                                traj_cut<D>(T, r0 + q, tt, cutoff, sbox[gl]);
-                            else
-                                closed_cut<D>(cull[q < RJ ? r0 + q : r0 + q - RJ], q < RJ ? (float)P.c : -(float)P.c,
-                                              ta, tb, P, cutoff, sbox[gl]);
-                        }
                         Rec<D> r;
                         if (g0 + gl < nsurv && tloc < t_cnt) {
                             const int q = surv[g0 + gl];
@@ -1045,29 +926,15 @@ adj32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
                     const int ng = min(G, nsurv - g0);
                     for (int gl = 0; gl < ng; gl += 2) {
                         float2 ar = make_float2(0.0f, 0.0f), ai = make_float2(0.0f, 0.0f);
-                        // the pair against this warp's group (warp-uniform)
-                        const bool ua = active && cut_near<D>(sbox[gl], gi, cutoff);
-                        const bool ub = active && gl + 1 < ng && cut_near<D>(sbox[gl + 1], gi, cutoff);
-                        if (ua || ub) {
-                            if (lane == 0) evals += (unsigned long long)(ua + ub) * g_evals;
+                        if (active) {
                             Rec<D> ra, rb;
                             load_rec<D>(rec, gl, lane, ra);
                             load_rec<D>(rec, gl + 1, lane, rb);  // zero-amplitude record when gl + 1 == ng
-                            if (!ua) ra.amp = 0.0f;
-                            if (!ub) rb.amp = 0.0f;
                             cf za, fa, qa, zb, fb, qb;
                             int ka = kRunRecurrence, kb = kRunRecurrence;
                             if (fast) {
-                                if (ua)
-                                    za = seed_eval<D, false>(ra, sds[gbase], shn[gbase], true, P, fa, qa, &ka,
-                                                             cutoff > 0.0f);
-                                else
-                                    ka = kRunNegligible;
-                                if (ub)
-                                    zb = seed_eval<D, false>(rb, sds[gbase], shn[gbase], true, P, fb, qb, &kb,
-                                                             cutoff > 0.0f);
-                                else
-                                    kb = kRunNegligible;
+                                za = seed_eval<D, false>(ra, sds[gbase], shn[gbase], true, P, fa, qa, &ka, cutoff > 0.0f);
+                                zb = seed_eval<D, false>(rb, sds[gbase], shn[gbase], true, P, fb, qb, &kb, cutoff > 0.0f);
                                 if (ka == kRunNegligible) za = fa = qa = cf{0.0f, 0.0f};
                                 if (kb == kRunNegligible) zb = fb = qb = cf{0.0f, 0.0f};
                             }
@@ -1115,15 +982,15 @@ adj32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
                                     ai.y = fmaf(-d, zb.im, ai.y);
                                 }
                             }
-                            // over the 32 times: paired FP32 adds (the partials are sums of
-                            // 16 terms; FP64 from here on)
+                        }
+                        // over the 32 times: paired FP32 adds (the partials are sums of
+                        // 16 terms; FP64 from here on)
 #pragma unroll
-                            for (int o = 16; o > 0; o >>= 1) {
-                                ar = __fadd2_rn(ar, make_float2(__shfl_xor_sync(0xffffffffu, ar.x, o),
-                                                                __shfl_xor_sync(0xffffffffu, ar.y, o)));
-                                ai = __fadd2_rn(ai, make_float2(__shfl_xor_sync(0xffffffffu, ai.x, o),
-                                                                __shfl_xor_sync(0xffffffffu, ai.y, o)));
-                            }
+                        for (int o = 16; o > 0; o >>= 1) {
+                            ar = __fadd2_rn(ar, make_float2(__shfl_xor_sync(0xffffffffu, ar.x, o),
+                                                            __shfl_xor_sync(0xffffffffu, ar.y, o)));
+                            ai = __fadd2_rn(ai, make_float2(__shfl_xor_sync(0xffffffffu, ai.x, o),
+                                                            __shfl_xor_sync(0xffffffffu, ai.y, o)));
                         }
                         if (lane == 0) {
                             wpart[warp][gl][0] = (double)ar.x;
@@ -1164,7 +1031,7 @@ adj32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
             acc_smem[2 * q + 1] = 0.0;
         }
     }
-    if (eval_count && lane == 0 && evals) atomicAdd(eval_count, evals);  // per warp: its group's evaluations
+    if (eval_count && tid == 0 && evals) atomicAdd(eval_count, evals);
 }
 
 // g[j] = sum over time tiles, in order, of part[tt][j] (trajectories) or of
