@@ -179,9 +179,11 @@ __global__ void __launch_bounds__(GT) gemm_tc_kernel(GemmArgs g) {
 //   warp 1   - one lane issues tcgen05.mma (M = 128, N, K = 16 per
 //              instruction) into one of two TMEM accumulators (2 x 256
 //              columns) and commits each stage back to the ring;
-//   warps 2-5 - the epilogue: tcgen05.ld of their 32 TMEM lanes, bias, SiLU,
-//              FP32 / BF16 stores, then release the accumulator, so the MMAs
-//              of the next tile overlap this tile's epilogue.
+//   warps 2-9 - the epilogue, two warps per quarter of the TMEM lanes (a
+//              warp reads only its own quarter), each taking every other
+//              16-column chunk: tcgen05.ld, bias, SiLU, FP32 / BF16 stores,
+//              then release the accumulator, so the MMAs of the next tile
+//              overlap this tile's epilogue.
 // Operands use the 128-byte swizzle (TMA box rows of 64 BF16 = 128 B); the
 // UMMA descriptors address 8-row atoms of 1024 B (SBO) and advance 32 B per
 // K = 16 step inside the swizzled row.  Every mbarrier wait is bounded: on
@@ -191,7 +193,7 @@ constexpr int TG_BM = 128;
 constexpr int TG_BK = 64;
 constexpr int TG_STAGES = 4;
 constexpr int TG_MAXKB = 4;  // K <= 256
-constexpr int TG_THREADS = 192;
+constexpr int TG_THREADS = 320;
 constexpr uint32_t TG_A_STAGE = TG_BM * TG_BK * 2;  // 16 KB
 constexpr size_t TG_SMEM = (size_t)TG_STAGES * TG_A_STAGE + (size_t)TG_MAXKB * 256 * TG_BK * 2 + 256 + 1024;
 
@@ -267,7 +269,7 @@ gemm_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b_full));
         for (int a = 0; a < 2; ++a) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tfull(a)));
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(tempty(a)));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 8;" ::"r"(tempty(a)));
         }
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mma_done));
         *abort = 0;
@@ -376,7 +378,8 @@ gemm_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             mbar_wait(mma_done, 0, &never);
         }
     } else {
-        const int quarter = warp & 3;  // TMEM lanes 32 quarter .. + 31
+        const int quarter = warp & 3;         // TMEM lanes 32 quarter .. + 31
+        const int half = (warp - 2) >> 2;     // 16-column chunks half, half + 2, ...
         const bool vec32 = g.C32 && (g.ldc32 & 3) == 0 && ((uintptr_t)g.C32 & 15) == 0;
         const bool vec16 = g.C16 && (g.ldc16 & 7) == 0 && ((uintptr_t)g.C16 & 15) == 0;
         bool ok = true;
@@ -389,7 +392,7 @@ gemm_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             if (!ok) break;
             asm volatile("tcgen05.fence::after_thread_sync;");
             const int row = m0 + 32 * quarter + lane;
-            for (int col0 = 0; col0 < g.N; col0 += 16) {
+            for (int col0 = 16 * half; col0 < g.N; col0 += 32) {
                 uint32_t r[16];
                 const uint32_t taddr = tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(a * 256 + col0);
                 asm volatile(

@@ -149,8 +149,10 @@ __device__ void rhs_sym(const MediumArgs &med, double mode, const SState<D> &y, 
     double n2 = 0.0;
 #pragma unroll
     for (int i = 0; i < D; ++i) n2 += y.p[i] * y.p[i];
-    const double np = sqrt(n2);
-    const double inp = 1.0 / np;
+    // FP32 path: 1/|p| from the FP64 reciprocal square root (one rounding
+    // step from sqrt then divide, at a fraction of their instructions)
+    const double inp = F32M ? rsqrt(n2) : 1.0 / sqrt(n2);
+    const double np = F32M ? n2 * inp : sqrt(n2);
     const double inp3 = inp * inp * inp;
     const double G = mode * c * np;
     double Gx[D], Gp[D];
@@ -204,7 +206,10 @@ __device__ void rhs_sym(const MediumArgs &med, double mode, const SState<D> &y, 
     }
     cd num = (c * c) * trM;
     num = cd{num.re - gxgp - gpmgp.re + med.lam * G, num.im - gpmgp.im};
-    const cd f = (-1.0 / (2.0 * G)) * num;
+    // -1 / (2 G) = -mode / (2 c |p|); the FP32 path takes 1/c in FP32 (the
+    // amplitude's rate to FP32 precision, as its medium evaluation)
+    const double ig = F32M ? -0.5 * mode * inp * (double)__frcp_rn((float)c) : -1.0 / (2.0 * G);
+    const cd f = ig * num;
     dy.A = y.A * f;
 }
 
@@ -400,8 +405,8 @@ struct DopriBeam {
         }
 #define KSV(j, c) ks[((j) * N + (c)) * kst]
         // yt now holds the 5th-order solution (stage 7's input).
-        double sum = 0.0;
         const double *nv = vals(yt);
+        double err;
         {
             double ev[N];
 #pragma unroll
@@ -411,21 +416,35 @@ struct DopriBeam {
                 ev[c] = hh * acc;
             }
             // (|e| / (atol + rtol max(|y0|, |y1|)))^2 from squared magnitudes:
-            // one square root per entry instead of three
+            // one square root per entry instead of three.  The FP32 path
+            // forms the norm, a step-size heuristic, in FP32.
+            if (F32M) {
+                const float at = (float)o.atol, rt = (float)o.rtol;
+                float s32 = 0.0f;
 #pragma unroll
-            for (int e = 0; e < NE; ++e) {
-                const double sc = o.atol + o.rtol * sqrt(fmax(entry_abs2<D>(yv, e), entry_abs2<D>(nv, e)));
-                sum += sym_weight<D>(e) * (entry_abs2<D>(ev, e) / (sc * sc));
+                for (int e = 0; e < NE; ++e) {
+                    const float sc = fmaf(rt, sqrtf((float)fmax(entry_abs2<D>(yv, e), entry_abs2<D>(nv, e))), at);
+                    s32 = fmaf((float)sym_weight<D>(e), __fdividef((float)entry_abs2<D>(ev, e), sc * sc), s32);
+                }
+                err = (double)sqrtf(s32 * (1.0f / NE_FULL));
+            } else {
+                double sum = 0.0;
+#pragma unroll
+                for (int e = 0; e < NE; ++e) {
+                    const double sc = o.atol + o.rtol * sqrt(fmax(entry_abs2<D>(yv, e), entry_abs2<D>(nv, e)));
+                    sum += sym_weight<D>(e) * (entry_abs2<D>(ev, e) / (sc * sc));
+                }
+                err = sqrt(sum / NE_FULL);
             }
         }
-        const double err = sqrt(sum / NE_FULL);
         ++steps;
         if (!isfinite(err)) {
             h = 0.2 * hh;
             rejected = true;
             return false;
         }
-        double fac = err == 0.0 ? 10.0 : fmin(10.0, fmax(0.2, 0.9 * pow(err, -0.2)));
+        const double gr = F32M ? (double)(0.9f * exp2f(-0.2f * log2f((float)err))) : 0.9 * pow(err, -0.2);
+        double fac = err == 0.0 ? 10.0 : fmin(10.0, fmax(0.2, gr));
         if (err <= 1.0) {
             if (rejected) fac = fmin(fac, 1.0);
             rejected = false;

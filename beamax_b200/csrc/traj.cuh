@@ -30,6 +30,12 @@ __device__ __forceinline__ int map_index(int i, int n, int boundary) {
     }
 }
 
+// Tap k of the `taps` consecutive taps starting at lo: inside the grid (the
+// usual case) the index itself, else the boundary rule.
+__device__ __forceinline__ int tap_index(int lo, int k, int taps, int n, int boundary) {
+    return (lo >= 0 && lo + taps <= n) ? lo + k : map_index(lo + k, n, boundary);
+}
+
 // c, grad c (D), hess c (D x D, row-major) at x, for a medium of kind KIND
 // (the tap count and the weights are then compile-time constants).
 template <int D, int KIND>
@@ -80,7 +86,7 @@ __device__ __forceinline__ void speed_eval_k(const MediumArgs &m, const double *
             w[a][2] = w[a][3] = d1[a][2] = d1[a][3] = d2[a][2] = d2[a][3] = 0.0;
         }
 #pragma unroll
-        for (int k = 0; k < taps; ++k) idx[a][k] = map_index(i0 + off0 + k, m.n[a], m.boundary);
+        for (int k = 0; k < taps; ++k) idx[a][k] = tap_index(i0 + off0, k, taps, m.n[a], m.boundary);
     }
     // Separable reduction, last axis first: the tensor-product weights factor,
     // so the value, gradient and Hessian need 3 sums per line of the last
@@ -218,7 +224,7 @@ __device__ __forceinline__ void speed_eval_f32(const MediumArgs &m, const double
             w[a][2] = w[a][3] = d1[a][2] = d1[a][3] = d2[a][2] = d2[a][3] = 0.0f;
         }
 #pragma unroll
-        for (int k = 0; k < taps; ++k) idx[a][k] = map_index(i0 + off0 + k, m.n[a], m.boundary);
+        for (int k = 0; k < taps; ++k) idx[a][k] = tap_index(i0 + off0, k, taps, m.n[a], m.boundary);
     }
     float cc = 0.0f, gg[D], hh[D][D];
 #pragma unroll
