@@ -420,11 +420,13 @@ def run_ours(args, rank, world, device):
 def run_ode_only(args, device, peaks):
     """The beam ODE alone (``--ode-only``): the workload's selection, then
     msgb_ode_trajectories over every beam (both modes) writing the FP32
-    summation records and culling boxes, in the chunks the solver uses; W
-    untimed and K timed integrations, CUDA events on the launching stream."""
+    summation records into the compact store, in the chunks the solver's
+    forward uses; W untimed and K timed integrations, CUDA events on the
+    launching stream."""
     import torch
 
     import beamax_b200 as bb
+    from beamax_b200 import _lib
 
     torch.cuda.set_device(device)
     W = WORKLOADS[args.workload](seed=1234, thr=args.thr)
@@ -439,13 +441,16 @@ def run_ode_only(args, device, peaks):
     med, keep_m = s._medium(dom, device)
     bs = bt.beam_set(unit=False)
     st = torch.cuda.current_stream(device)
-    chunks, per, n_tt = s._mode_chunks(dom, pr.nt, bt, False)
     status = torch.zeros(2 * bt.n, dtype=torch.int32, device=device)
     ctr = torch.zeros(1, dtype=torch.int64, device=device)
+    tiling = s._tiling(dom, sens, device)
+    sopts = _lib.SumOpts(cutoff=s.cutoff, tiling=_lib.ref(tiling[0]) if tiling else None)
+    n_chunks = [0]
 
     def integrate():
-        for b_first, nb in chunks:
-            s._trajectories(pr, med, bs, b_first, nb, False, per, n_tt, device, st.cuda_stream, status)
+        n_chunks[0] = 0
+        for _ in s._compact_integrate(pr, med, bs, 0, 2 * bt.n, dom, sens, sopts, device, st.cuda_stream, status):
+            n_chunks[0] += 1
 
     for _ in range(max(args.warmup, 1)):
         integrate()
@@ -461,7 +466,7 @@ def run_ode_only(args, device, peaks):
     steps = int(ctr.item()) / args.steps
     fl = ode_flops_per_step(len(dom.N))
     achieved = steps * fl / secs / 1e12
-    line = {"mode": "ode_only", "workload": W["name"], "beams": 2 * bt.n, "nt": pr.nt, "chunks": len(chunks),
+    line = {"mode": "ode_only", "workload": W["name"], "beams": 2 * bt.n, "nt": pr.nt, "chunks": n_chunks[0],
             "ode_s": secs, "attempted_steps": steps, "steps_per_beam": steps / (2 * bt.n),
             "beam_steps_per_s": steps / secs, "flops_per_step": fl, "achieved_tflops": achieved,
             "peak_fp64_tflops": peaks["fp64"] if peaks else None,
