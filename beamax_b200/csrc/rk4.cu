@@ -323,6 +323,13 @@ template <int D>
 constexpr size_t dopri_smem_bytes(int blk) {
     return (size_t)blk * 7 * NVS<D>::value * sizeof(double);
 }
+// The mixed-precision integrator's: 7 FP64 ray stages and 7 FP32 Hessian and
+// amplitude stages per lane (28 KB per 64 lanes in 2D, 46.6 KB in 3D).
+template <int D>
+constexpr size_t dopri_mix_smem_bytes(int blk) {
+    return (size_t)blk * 7 * (2 * D * sizeof(double) + (D * (D + 1) + 2) * sizeof(float));
+}
+constexpr int kMixBlocks = 6;  // default blocks per SM of the mixed-precision integrator
 
 // DENSE: save times may fall inside a step (msgb_ode_opts.dense_output);
 // without it every step ends on a save time and the continuous extension is
@@ -491,6 +498,311 @@ struct DopriBeam {
     }
 };
 
+// ---- the FP32 path's mixed-precision integrator ------------------------------
+// The ray (x, p) stays FP64: the summation's phase w p.(s - x) needs it.  The
+// Hessian M and the amplitude A, which enter the FP32 summation as FP32
+// values, are integrated in FP32 with the same Dormand-Prince stages and the
+// same error control (their FP32 rounding, ~1e-7 relative per step, stays far
+// below the FP32 path's 1e-3 budget).  Half the FP64 dependency chains, 2/3 of
+// the stage memory and fewer registers than DopriBeam.
+template <int D>
+struct MState {
+    static constexpr int S = D * (D + 1) / 2;
+    static constexpr int ND = 2 * D;      // doubles: x, p
+    static constexpr int NF = 2 * S + 2;  // floats: M (re, im) in sym_index order, A (re, im)
+    double r[ND];
+    float f[NF];
+};
+
+template <int D>
+__device__ __forceinline__ void mix_to_full(const MState<D> &s, State<D> &o) {
+    constexpr int S = MState<D>::S;
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+        o.x[i] = s.r[i];
+        o.p[i] = s.r[D + i];
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            const int q = sym_index<D>(i, k);
+            o.M[i][k] = cd{(double)s.f[2 * q], (double)s.f[2 * q + 1]};
+        }
+    }
+    o.A = cd{(double)s.f[2 * S], (double)s.f[2 * S + 1]};
+}
+
+template <int D>
+__device__ __forceinline__ void mix_from_full(const State<D> &o, MState<D> &s) {
+    constexpr int S = MState<D>::S;
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+        s.r[i] = o.x[i];
+        s.r[D + i] = o.p[i];
+#pragma unroll
+        for (int k = i; k < D; ++k) {
+            const int q = sym_index<D>(i, k);
+            s.f[2 * q] = (float)o.M[i][k].re;
+            s.f[2 * q + 1] = (float)o.M[i][k].im;
+        }
+    }
+    s.f[2 * S] = (float)o.A.re;
+    s.f[2 * S + 1] = (float)o.A.im;
+}
+
+// coupled_rhs_absorption: the ray terms in FP64, the Riccati and amplitude
+// terms in FP32 (the same terms as rhs_sym).
+template <int D, int KIND>
+__device__ void rhs_mix(const MediumArgs &med, double mode, const MState<D> &y, MState<D> &dy) {
+    constexpr int S = MState<D>::S;
+    double c, gc[D], hc[D * D];
+    if (KIND != MSGB_MEDIUM_CONSTANT)
+        speed_eval_f32<D, KIND>(med, y.r, c, gc, hc);
+    else
+        speed_eval_k<D, KIND>(med, y.r, c, gc, hc);
+    const double *p = y.r + D;
+    double n2 = 0.0;
+#pragma unroll
+    for (int i = 0; i < D; ++i) n2 += p[i] * p[i];
+    const double inp = rsqrt(n2);
+    const double np = n2 * inp;
+    const double mc_inp = mode * c * inp, mnp = mode * np;
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+        dy.r[i] = mc_inp * p[i];     // G_p
+        dy.r[D + i] = -mnp * gc[i];  // -G_x
+    }
+    const float m = (float)mode, cf = (float)c, npf = (float)np, inpf = (float)inp;
+    const float inp3 = inpf * inpf * inpf;
+    float pf[D], Gx[D], Gp[D];
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+        pf[i] = (float)p[i];
+        Gp[i] = (float)dy.r[i];
+        Gx[i] = -(float)dy.r[D + i];
+    }
+    float Gpp[D][D], Gxp[D][D];
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            Gpp[i][k] = m * cf * ((i == k ? inpf : 0.0f) - pf[i] * pf[k] * inp3);
+            Gxp[i][k] = Gx[i] * pf[k] * inpf * inpf;  // m gc_i |p| p_k / |p|^2 = m gc_i p_k / |p|
+        }
+    auto Mre = [&](int i, int k) { return y.f[2 * sym_index<D>(i, k)]; };
+    auto Mim = [&](int i, int k) { return y.f[2 * sym_index<D>(i, k) + 1]; };
+    float MGr[D][D], MGi[D][D];
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            float sr = 0.0f, si = 0.0f;
+#pragma unroll
+            for (int l = 0; l < D; ++l) {
+                sr = fmaf(Gpp[l][k], Mre(i, l), sr);
+                si = fmaf(Gpp[l][k], Mim(i, l), si);
+            }
+            MGr[i][k] = sr;
+            MGi[i][k] = si;
+        }
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int k = i; k < D; ++k) {
+            float sr = m * (float)hc[i * D + k] * npf, si = 0.0f;
+#pragma unroll
+            for (int l = 0; l < D; ++l) {
+                sr = fmaf(Gxp[i][l], Mre(l, k), sr);
+                si = fmaf(Gxp[i][l], Mim(l, k), si);
+                sr = fmaf(Gxp[k][l], Mre(i, l), sr);
+                si = fmaf(Gxp[k][l], Mim(i, l), si);
+                // (MG)_il M_lk, complex
+                sr = fmaf(MGr[i][l], Mre(l, k), fmaf(-MGi[i][l], Mim(l, k), sr));
+                si = fmaf(MGr[i][l], Mim(l, k), fmaf(MGi[i][l], Mre(l, k), si));
+            }
+            const int q = sym_index<D>(i, k);
+            dy.f[2 * q] = -sr;
+            dy.f[2 * q + 1] = -si;
+        }
+    float trr = 0.0f, tri = 0.0f, gxgp = 0.0f, gmr = 0.0f, gmi = 0.0f;
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+        trr += Mre(i, i);
+        tri += Mim(i, i);
+        gxgp = fmaf(Gx[i], Gp[i], gxgp);
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            const float gg = Gp[i] * Gp[k];
+            gmr = fmaf(gg, Mre(i, k), gmr);
+            gmi = fmaf(gg, Mim(i, k), gmi);
+        }
+    }
+    const float c2 = cf * cf;
+    const float nr = fmaf(c2, trr, -gxgp) - gmr + (float)med.lam * (m * cf * npf);
+    const float ni = fmaf(c2, tri, -gmi);
+    // -1 / (2 G) = -mode / (2 c |p|)
+    const float ig = -0.5f * m * inpf * __frcp_rn(cf);
+    const float fr = ig * nr, fi = ig * ni;
+    const float ar = y.f[2 * S], ai = y.f[2 * S + 1];
+    dy.f[2 * S] = fmaf(ar, fr, -ai * fi);
+    dy.f[2 * S + 1] = fmaf(ar, fi, ai * fr);
+}
+
+__constant__ float DP_A32[7][6] = {
+    {0, 0, 0, 0, 0, 0},
+    {(float)(1.0 / 5), 0, 0, 0, 0, 0},
+    {(float)(3.0 / 40), (float)(9.0 / 40), 0, 0, 0, 0},
+    {(float)(44.0 / 45), (float)(-56.0 / 15), (float)(32.0 / 9), 0, 0, 0},
+    {(float)(19372.0 / 6561), (float)(-25360.0 / 2187), (float)(64448.0 / 6561), (float)(-212.0 / 729), 0, 0},
+    {(float)(9017.0 / 3168), (float)(-355.0 / 33), (float)(46732.0 / 5247), (float)(49.0 / 176),
+     (float)(-5103.0 / 18656), 0},
+    {(float)(35.0 / 384), 0, (float)(500.0 / 1113), (float)(125.0 / 192), (float)(-2187.0 / 6784), (float)(11.0 / 84)}};
+__constant__ float DP_E32[7] = {(float)(35.0 / 384 - 5179.0 / 57600),
+                                0.0f,
+                                (float)(500.0 / 1113 - 7571.0 / 16695),
+                                (float)(125.0 / 192 - 393.0 / 640),
+                                (float)(-2187.0 / 6784 + 92097.0 / 339200),
+                                (float)(11.0 / 84 - 187.0 / 2100),
+                                (float)(-1.0 / 40)};
+
+// DopriBeam's step (save times landed on, no continuous extension) on the
+// mixed state.  Stages in shared memory: the FP64 ray stages, then the FP32
+// Hessian and amplitude stages, each entry strided by the block size.
+template <int D, int KIND>
+struct DopriMix {
+    static constexpr int ND = MState<D>::ND, NF = MState<D>::NF, S = MState<D>::S;
+    MState<D> y;
+    double t, h, mode;
+    int64_t steps, k;
+    bool rejected;
+    int code;
+    double *k64;  // stage j, entry c at k64[(j ND + c) kst]
+    float *k32;   // stage j, entry c at k32[(j NF + c) kst]
+    int kst;
+
+    __device__ void init(const MediumArgs &med, const ProbArgs &P, const OdeArgs &o, double mode_) {
+        mode = mode_;
+        h = o.dt0 > 0.0 ? o.dt0 : (P.nt > 1 ? P.ts[1] - P.ts[0] : 0.0);
+        t = P.ts[0];
+        steps = 0;
+        k = 1;
+        rejected = false;
+        code = 0;
+        MState<D> f0;
+        rhs_mix<D, KIND>(med, mode, y, f0);
+#pragma unroll
+        for (int c = 0; c < ND; ++c) k64[c * kst] = f0.r[c];
+#pragma unroll
+        for (int c = 0; c < NF; ++c) k32[c * kst] = f0.f[c];
+    }
+
+    __device__ bool attempt(const MediumArgs &med, const ProbArgs &P, const OdeArgs &o, RecordWriter<D> &rw) {
+        constexpr int NE = 2 * D + S + 1;          // entries of the error norm (x, p real; M, A complex)
+        constexpr int NE_FULL = 2 * D + D * D + 1;  // entries of the full state
+        if (k >= P.nt) return true;
+        if (steps >= o.max_steps + P.nt - 1) {
+            code = 2;
+            return true;
+        }
+        const double target = P.ts[k];
+        double hh = h;
+        bool last = false;
+        if (t + hh >= target) {
+            hh = target - t;
+            last = true;
+        }
+        const float hf = (float)hh;
+        MState<D> yt;
+#pragma unroll 1
+        for (int s = 1; s < 7; ++s) {
+            double a64[ND];
+            float a32[NF];
+#pragma unroll
+            for (int c = 0; c < ND; ++c) a64[c] = 0.0;
+#pragma unroll
+            for (int c = 0; c < NF; ++c) a32[c] = 0.0f;
+#pragma unroll 1
+            for (int j = 0; j < s; ++j) {
+                const double a = DP_A[s][j];
+                if (a != 0.0) {
+                    const float af = DP_A32[s][j];
+#pragma unroll
+                    for (int c = 0; c < ND; ++c) a64[c] += a * k64[(j * ND + c) * kst];
+#pragma unroll
+                    for (int c = 0; c < NF; ++c) a32[c] = fmaf(af, k32[(j * NF + c) * kst], a32[c]);
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < ND; ++c) yt.r[c] = y.r[c] + hh * a64[c];
+#pragma unroll
+            for (int c = 0; c < NF; ++c) yt.f[c] = fmaf(hf, a32[c], y.f[c]);
+            MState<D> kn;
+            rhs_mix<D, KIND>(med, mode, yt, kn);
+#pragma unroll
+            for (int c = 0; c < ND; ++c) k64[(s * ND + c) * kst] = kn.r[c];
+#pragma unroll
+            for (int c = 0; c < NF; ++c) k32[(s * NF + c) * kst] = kn.f[c];
+        }
+        // yt holds the 5th-order solution.  Error norm in FP32, as DopriBeam's
+        // FP32-path variant forms it.
+        float s32 = 0.0f;
+        {
+            const float at = (float)o.atol, rt = (float)o.rtol;
+#pragma unroll
+            for (int c = 0; c < ND; ++c) {
+                double acc = 0.0;
+                for (int j = 0; j < 7; ++j) acc += DP_E[j] * k64[(j * ND + c) * kst];
+                const float e = (float)(hh * acc);
+                const float sc = fmaf(rt, (float)fmax(fabs(y.r[c]), fabs(yt.r[c])), at);
+                s32 = fmaf(e, __fdividef(e, sc * sc), s32);
+            }
+#pragma unroll
+            for (int q = 0; q < S + 1; ++q) {
+                float er = 0.0f, ei = 0.0f;
+                for (int j = 0; j < 7; ++j) {
+                    er = fmaf(DP_E32[j], k32[(j * NF + 2 * q) * kst], er);
+                    ei = fmaf(DP_E32[j], k32[(j * NF + 2 * q + 1) * kst], ei);
+                }
+                er *= hf;
+                ei *= hf;
+                const float y0 = fmaf(y.f[2 * q], y.f[2 * q], y.f[2 * q + 1] * y.f[2 * q + 1]);
+                const float y1 = fmaf(yt.f[2 * q], yt.f[2 * q], yt.f[2 * q + 1] * yt.f[2 * q + 1]);
+                const float sc = fmaf(rt, sqrtf(fmaxf(y0, y1)), at);
+                s32 = fmaf((float)sym_weight<D>(2 * D + q), __fdividef(fmaf(er, er, ei * ei), sc * sc), s32);
+            }
+        }
+        const float err = sqrtf(s32 * (1.0f / NE_FULL));
+        (void)NE;
+        ++steps;
+        if (!isfinite(err)) {
+            h = 0.2 * hh;
+            rejected = true;
+            return false;
+        }
+        double fac = err == 0.0f ? 10.0 : fmin(10.0, fmax(0.2, (double)(0.9f * exp2f(-0.2f * log2f(err)))));
+        if (err <= 1.0f) {
+            if (rejected) fac = fmin(fac, 1.0);
+            rejected = false;
+            const double t_new = last ? target : t + hh;
+            while (k < P.nt && P.ts[k] <= t_new) {
+                State<D> yf;
+                mix_to_full(yt, yf);
+                rw.put(k, yf, false);
+                ++k;
+            }
+            t = t_new;
+            y = yt;
+#pragma unroll
+            for (int c = 0; c < ND; ++c) k64[c * kst] = k64[(6 * ND + c) * kst];  // first same as last
+#pragma unroll
+            for (int c = 0; c < NF; ++c) k32[c * kst] = k32[(6 * NF + c) * kst];
+            h = last ? fmax(hh * fac, h) : hh * fac;
+        } else {
+            h = hh * fmin(1.0, fac);
+            rejected = true;
+        }
+        return k >= P.nt;
+    }
+};
+
 template <int D>
 __device__ void launch_state(const BeamArgs &B, const TrajArgs &T, int64_t bl, State<D> &y, double &mode, double &w) {
     const int64_t b = T.b_first + bl;
@@ -549,6 +861,59 @@ dopri_kernel(ProbArgs P, MediumArgs med, BeamArgs B, TrajArgs T, OdeArgs o, int 
             if (s.k < P.nt) {  // after a failure: the last state
                 State<D> yf;
                 to_full(s.y, yf);
+                for (int64_t k = s.k; k < P.nt; ++k) rw.put(k, yf, true);
+            }
+            if (T.status) T.status[bl] = s.code;
+            lane_steps += (unsigned long long)s.steps;
+            active = false;
+        }
+    }
+    if (o.step_count) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) lane_steps += __shfl_xor_sync(0xffffffffu, lane_steps, off);
+        if ((threadIdx.x & 31) == 0 && lane_steps) atomicAdd(o.step_count, lane_steps);
+    }
+}
+
+// dopri_kernel with the FP32 path's mixed-precision state (DopriMix).
+template <int D, int KIND, int MINB>
+__global__ void __launch_bounds__(64, MINB)
+dopri_mix_kernel(ProbArgs P, MediumArgs med, BeamArgs B, TrajArgs T, OdeArgs o, int tt_len) {
+    constexpr int ND = MState<D>::ND;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t bl = blockIdx.x * (int64_t)blockDim.x + threadIdx.x - stride;
+    bool active = false;
+    DopriMix<D, KIND> s;
+    s.k64 = dopri_stage_smem + threadIdx.x;
+    s.k32 = reinterpret_cast<float *>(dopri_stage_smem + 7 * ND * blockDim.x) + threadIdx.x;
+    s.kst = blockDim.x;
+    RecordWriter<D> rw(P, T, 0, 0.0, tt_len);
+    unsigned long long lane_steps = 0;
+    for (;;) {
+        if (!active) {
+            bl += stride;
+            while (bl < T.nb && o.only_flagged && T.status[bl] == 0) bl += stride;  // already accepted
+            if (bl < T.nb) {
+                double mode, w;
+                State<D> y0;
+                launch_state<D>(B, T, bl, y0, mode, w);
+                mix_from_full(y0, s.y);
+                rw.reset(bl, w);
+                rw.put(0, y0, false);
+                s.init(med, P, o, mode);
+                active = true;
+            }
+        }
+        if (!__any_sync(0xffffffffu, active)) break;
+        if (active && s.attempt(med, P, o, rw)) {
+            constexpr int S = MState<D>::S;
+            bool fin = isfinite(s.y.f[2 * S]) && isfinite(s.y.f[2 * S + 1]);
+#pragma unroll
+            for (int c = 0; c < ND; ++c) fin = fin && isfinite(s.y.r[c]);
+            if (!fin && s.code == 0) s.code = 1;
+            if (s.k < P.nt) {  // after a failure: the last state
+                State<D> yf;
+                mix_to_full(s.y, yf);
                 for (int64_t k = s.k; k < P.nt; ++k) rw.put(k, yf, true);
             }
             if (T.status) T.status[bl] = s.code;
@@ -658,34 +1023,45 @@ __global__ void tr_final_kernel(ProbArgs P, MediumArgs med, TrBeamsView B, int64
 // template argument).
 struct Dopri {
     int minb;
-    bool f32m;   // FP32 evaluation of the medium
+    bool f32m;   // FP32 path: FP32 medium, and without dense output the mixed-precision state
     bool dense;  // save times from the continuous extension
+    bool mixed() const { return f32m && !dense; }
     template <int D, int K>
     auto kernel() const {
         if (dense) return f32m ? dopri_kernel<D, K, 4, true, true> : dopri_kernel<D, K, 4, false, true>;
-        if (f32m) return minb >= 5 ? dopri_kernel<D, K, 5, true, false> : dopri_kernel<D, K, 4, true, false>;
+        if (f32m)
+            return minb >= 7   ? dopri_mix_kernel<D, K, 7>
+                   : minb == 6 ? dopri_mix_kernel<D, K, 6>
+                   : minb == 5 ? dopri_mix_kernel<D, K, 5>
+                               : dopri_mix_kernel<D, K, 4>;
         return minb >= 5 ? dopri_kernel<D, K, 5, false, false> : dopri_kernel<D, K, 4, false, false>;
     }
+    template <int D>
+    size_t smem() const { return mixed() ? dopri_mix_smem_bytes<D>(64) : dopri_smem_bytes<D>(64); }
 };
 struct TrFinal {
     template <int D, int K>
     auto kernel() const { return tr_final_kernel<D, K>; }
+    template <int D>
+    size_t smem() const { return dopri_smem_bytes<D>(64); }
 };
 
-// Blocks per SM of the adaptive integrator: 4 (8 warps, up to 255 registers
-// per lane) unless MSGB_DOPRI_BLOCKS=5 (10 warps, registers bounded to 204).
-int dopri_blocks_per_sm() {
-    static const int v = [] {
+// Blocks of 64 lanes per SM of the adaptive integrator: MSGB_DOPRI_BLOCKS
+// (4 to 7; 5, 6 and 7 bound the registers to 204, 170 and 146; the FP64
+// integrator takes at most 5), else `dflt`.
+int dopri_blocks_per_sm(int dflt) {
+    static const int env = [] {
         const char *e = getenv("MSGB_DOPRI_BLOCKS");
-        return (e && atoi(e) == 5) ? 5 : 4;
+        const int v = e ? atoi(e) : 0;
+        return (v >= 4 && v <= 7) ? v : 0;
     }();
-    return v;
+    return env ? env : dflt;
 }
 
 template <int D, typename Launch, typename Which>
 void launch_by_kind(int kind, Launch launch, const Which &which) {
     auto go = [&](auto kern) {
-        const size_t smem = dopri_smem_bytes<D>(64);
+        const size_t smem = which.template smem<D>();
         if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         launch(kern, smem);
     };
@@ -787,11 +1163,18 @@ extern "C" int msgb_ode_trajectories(const msgb_problem *prob, const msgb_medium
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        const int minb = dopri_blocks_per_sm();
-        const int64_t want = (int64_t)minb * sms;
-        const unsigned grid = (unsigned)(need < want ? need : want);
         const bool f32m = opts->medium_fp32 != 0 && med->coeffs32 != nullptr && med->kind != MSGB_MEDIUM_CONSTANT;
-        const Dopri which{minb, f32m, opts->dense_output != 0};
+        Dopri which{4, f32m, opts->dense_output != 0};
+        which.minb = dopri_blocks_per_sm(which.mixed() ? kMixBlocks : 4);
+        if (!which.mixed() && which.minb > 5) which.minb = 5;
+        {
+            // the lanes are persistent: every block must be resident at once
+            const size_t sm_bytes = prob->ndim == 1 ? which.smem<1>() : (prob->ndim == 2 ? which.smem<2>() : which.smem<3>());
+            const int fit = (int)((size_t)(227 * 1024) / sm_bytes);
+            if (which.minb > fit) which.minb = fit < 4 ? 4 : fit;
+        }
+        const int64_t want = (int64_t)which.minb * sms;
+        const unsigned grid = (unsigned)(need < want ? need : want);
         switch (prob->ndim) {
             case 1: launch_by_kind<1>(M.kind, [&](auto kern, size_t sm) { kern<<<grid, blk, sm, st>>>(P, M, to_args(beams), T, O, MSGB_TIME_TILE); },
                                       which); break;

@@ -601,16 +601,16 @@ def rooflines(r, peaks, sm_mhz, args):
       FFMA2) and MUFU throughput of msgb_peak_probe.
     * Beam ODE (``dopri_kernel``): attempted Dormand-Prince steps counted on the
       device x ode_flops_per_step(d); peak: the measured DFMA throughput.
-    DRAM traffic per launch: the committed one-pass ncu capture for the
-    configuration-2 summation; null elsewhere (see profiles/)."""
+    DRAM traffic per launch: dram__bytes_read.sum + dram__bytes_write.sum of
+    the committed one-pass ncu capture of the workload at its default size
+    (profiles/dram_traffic_<workload>.json); null where there is none."""
     fp32 = peaks["fp32_best"] if peaks else 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
     basis32 = ("measured: " + peaks["method"]) if peaks else f"148 SM x 128 FP32 lanes x 2 x {sm_mhz:.0f} MHz"
     traffic = {}
-    prof = os.path.join(ROOT, "profiles", "fwd32_traffic_config2.json")
-    if os.path.exists(prof) and args.thr == 65536 and args.workload == "c2":
+    prof = os.path.join(ROOT, "profiles", f"dram_traffic_{args.workload}.json")
+    if os.path.exists(prof) and args.thr == DEFAULT_THR[args.workload]:
         with open(prof) as f:
-            t = json.load(f)
-        traffic = {"fwd": t.get("dram_bytes_per_launch"), "adj": t.get("adj32_dram_bytes_per_launch")}
+            traffic = json.load(f).get("per_launch_bytes", {})
     suffix = "<TRAJ>" if r["hetero"] else ""
     out = []
     for key, name, flops, evals, secs, what in (
@@ -620,7 +620,7 @@ def rooflines(r, peaks, sm_mhz, args):
             continue
         achieved = evals * flops / secs / 1e12
         entry = {"bound": "fp32", "achieved": achieved, "peak": fp32, "unit": "TFLOP/s",
-                 "frac": achieved / fp32, "traffic": traffic.get(key), "kernel": name + suffix,
+                 "frac": achieved / fp32, "traffic": traffic.get(name), "kernel": name + suffix,
                  "flops_per_eval": flops, "device_s_per_step": secs, "peak_basis": basis32,
                  "timing": f"CUDA events around the {what} entry point inside the timed steps "
                            "(device time per step, all chunks)"}
@@ -634,7 +634,7 @@ def rooflines(r, peaks, sm_mhz, args):
         achieved = r["ode_steps"] * fl / r["t_ode"] / 1e12
         peak = peaks["fp64"] if peaks else 148 * 64 * 2 * sm_mhz * 1e6 / 1e12
         out.append({"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                    "traffic": None, "kernel": "dopri_kernel", "flops_per_step": fl,
+                    "traffic": traffic.get("dopri_kernel"), "kernel": "dopri_kernel", "flops_per_step": fl,
                     "attempted_steps_per_step": r["ode_steps"], "device_s_per_step": r["t_ode"],
                     "peak_basis": ("measured: " + peaks["method"]) if peaks else
                                   f"148 SM x 64 FP64 lanes x 2 x {sm_mhz:.0f} MHz",
