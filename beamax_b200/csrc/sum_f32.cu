@@ -556,9 +556,11 @@ __device__ __forceinline__ void traj_beam_time(const BeamArgs &B, const TrajSrc<
         bt = T.rec[k * T.nb + bl];
     const int64_t b = T.b_first + bl;
     const int64_t j = b < B.n ? b : b - B.n;
-    const double ar = B.a0[2 * j], ai = B.a0[2 * j + 1];
-    bt.amp = (float)((double)bt.amp * hypot(ar, ai));
-    bt.ang = (float)((double)bt.ang + atan2(ai, (ar == 0.0 && ai == 0.0) ? 1e-12 : ar));
+    // the coefficient's amplitude and phase join the record's FP32 |A| and
+    // arg A in FP32 (the record already holds them to FP32 precision)
+    const float ar = (float)B.a0[2 * j], ai = (float)B.a0[2 * j + 1];
+    bt.amp *= hypotf(ar, ai);
+    bt.ang += atan2f(ai, (ar == 0.0f && ai == 0.0f) ? 1e-12f : ar);
 }
 
 // ------------------------------------------------------------------ forward
