@@ -329,7 +329,7 @@ template <int D>
 constexpr size_t dopri_mix_smem_bytes(int blk) {
     return (size_t)blk * 7 * (2 * D * sizeof(double) + (D * (D + 1) + 2) * sizeof(float));
 }
-constexpr int kMixBlocks = 7;  // default blocks per SM of the mixed-precision integrator (measured best in 2D)
+constexpr int kMixBlocks = 6;  // default blocks per SM of the mixed-precision integrator (measured best at config 3)
 
 // DENSE: save times may fall inside a step (msgb_ode_opts.dense_output);
 // without it every step ends on a save time and the continuous extension is

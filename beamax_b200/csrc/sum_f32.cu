@@ -41,6 +41,7 @@ constexpr int NW = 8;                // warps per CTA (forward)
 constexpr int TS = GS * NW;          // sensors per tile
 constexpr int THREADS = NW * 32;
 constexpr int G = THREADS / TT;      // beams per record pass
+static_assert(G % 2 == 0, "beams are evaluated in pairs");
 constexpr float kTwoPi = 6.283185307179586f;
 constexpr float kInvTwoPi = 0.15915494309189535f;
 
@@ -985,22 +986,22 @@ adj32_kernel(ProbArgs P, BeamArgs B, const Cull<D> *cull, const TileInfo<D> *til
                                 }
                             }
                         }
-                        // over the 32 times: paired FP32 adds (the partials are sums of
-                        // 16 terms; FP64 from here on)
-#pragma unroll
-                        for (int o = 16; o > 0; o >>= 1) {
-                            ar = __fadd2_rn(ar, make_float2(__shfl_xor_sync(0xffffffffu, ar.x, o),
-                                                            __shfl_xor_sync(0xffffffffu, ar.y, o)));
-                            ai = __fadd2_rn(ai, make_float2(__shfl_xor_sync(0xffffffffu, ai.x, o),
-                                                            __shfl_xor_sync(0xffffffffu, ai.y, o)));
-                        }
-                        if (lane == 0) {
-                            wpart[warp][gl][0] = (double)ar.x;
-                            wpart[warp][gl][1] = (double)ai.x;
-                            if (gl + 1 < G) {
-                                wpart[warp][gl + 1][0] = (double)ar.y;
-                                wpart[warp][gl + 1][1] = (double)ai.y;
-                            }
+                        // over the 32 times (the partials are sums of 16 terms): a
+                        // reduce-scatter of the pair's four partials, 6 shuffles
+                        // instead of 20.  Lanes 0, 8, 16, 24 end with the sums of
+                        // ar.x, ar.y, ai.x, ai.y; FP64 from here on.
+                        {
+                            const bool u4 = (lane & 16) != 0, u3 = (lane & 8) != 0;
+                            float k0 = u4 ? ai.x : ar.x, k1 = u4 ? ai.y : ar.y;
+                            k0 += __shfl_xor_sync(0xffffffffu, u4 ? ar.x : ai.x, 16);
+                            k1 += __shfl_xor_sync(0xffffffffu, u4 ? ar.y : ai.y, 16);
+                            float v = u3 ? k1 : k0;
+                            v += __shfl_xor_sync(0xffffffffu, u3 ? k0 : k1, 8);
+                            v += __shfl_xor_sync(0xffffffffu, v, 4);
+                            v += __shfl_xor_sync(0xffffffffu, v, 2);
+                            v += __shfl_xor_sync(0xffffffffu, v, 1);
+                            // beam gl + u3 (gl + 1 < G: gl is even and G is even), re / im by u4
+                            if ((lane & 7) == 0) wpart[warp][gl + (u3 ? 1 : 0)][u4 ? 1 : 0] = (double)v;
                         }
                     }
                     __syncthreads();

@@ -14,7 +14,8 @@ Synthetic seeded data of those shapes; nothing is downloaded.
 
 A step = one forward (p0 -> sensor data) plus one exact adjoint (data ->
 image) on the FP32 path (Kahan sums, FP64 anchor phases, Gaussian cutoff;
-beams integrated by the FP64 ODE).  The dense FP64 path (reference
+beams integrated once per step by the mixed-precision ODE: FP64 ray, FP32
+Hessian and amplitude).  The dense FP64 path (reference
 semantics: every beam at every time and sensor) is run once for comparison
 and as the accuracy reference.  ``value`` = dense-equivalent beam-sample
 evaluations per second of forward + adjoint (2 * 2n * Nt * Ns per step / step
@@ -414,6 +415,9 @@ def run_ours(args, rank, world, device):
         At = s32.adjoint(data_probe, dom, sens, ts, wpt, selection=s32.last_selection)
         lhs, rhs = float((Aq * data_probe).sum()), float((q * At).sum())
         result["dot_test_rel"] = abs(lhs - rhs) / abs(lhs)
+        # the same difference against |A q| |d|: independent of how small the
+        # inner product of the random probe with A q happens to be
+        result["dot_test_norm"] = abs(lhs - rhs) / float(torch.linalg.norm(Aq) * torch.linalg.norm(data_probe))
     return result
 
 
@@ -811,6 +815,7 @@ def main():
         line["rel_l2_fwd_vs_fp64"] = r["rel_l2_fwd"]
         line["rel_l2_adj_vs_fp64"] = r["rel_l2_adj"]
         line["dot_test_rel_fp32"] = r["dot_test_rel"]
+        line["dot_test_norm_fp32"] = r["dot_test_norm"]
     print(json.dumps(line), flush=True)
     return 0
 
