@@ -279,6 +279,18 @@ def ode_flops_per_step(d: int) -> float:
     return {2: 3624.0, 3: 9672.0}.get(d, 3624.0)
 
 
+def ode_flops_split(d: int):
+    """(FP64, FP32) flops of the same step in the FP32 path's mixed-precision
+    integrator, where only the ray is FP64: per right-hand side |p|^2, the
+    reciprocal square root, G_p and G_x (16 in 2D / 20 in 3D), and the stage
+    combinations and error estimate of the 2d ray entries (1/3 of the 840
+    flops of the 12-entry state in 2D, 6/20 of 1434 in 3D); everything else
+    (the medium, the Riccati and amplitude terms, their stages, the error
+    norm) is FP32."""
+    f64 = {2: 6 * 16 + 840 / 3, 3: 6 * 20 + 1434 * 6 / 20}.get(d, 6 * 16 + 840 / 3)
+    return f64, ode_flops_per_step(d) - f64
+
+
 # ---------------------------------------------------------------- ours
 def launches_per_step(levels: int) -> int:
     """Kernels of libmsgb launched per step (cuFFT's own kernels excluded)."""
@@ -634,14 +646,17 @@ def rooflines(r, peaks, sm_mhz, args):
                              "ops_per_eval": 3}
         out.append(entry)
     if r["hetero"] and r["t_ode"] > 0 and r["ode_steps"] > 0:
-        fl = ode_flops_per_step(r["ndim"])
-        achieved = r["ode_steps"] * fl / r["t_ode"] / 1e12
-        peak = peaks["fp64"] if peaks else 148 * 64 * 2 * sm_mhz * 1e6 / 1e12
-        out.append({"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                    "traffic": traffic.get("dopri_kernel"), "kernel": "dopri_kernel", "flops_per_step": fl,
+        # the FP32 path's mixed-precision integrator: FP32 for all but the ray
+        f64, f32 = ode_flops_split(r["ndim"])
+        rate = r["ode_steps"] / r["t_ode"]
+        peak64 = peaks["fp64"] if peaks else 148 * 64 * 2 * sm_mhz * 1e6 / 1e12
+        a32, a64 = rate * f32 / 1e12, rate * f64 / 1e12
+        out.append({"bound": "fp32", "achieved": a32, "peak": fp32, "unit": "TFLOP/s", "frac": a32 / fp32,
+                    "fp64": {"achieved": a64, "peak": peak64, "frac": a64 / peak64, "flops_per_step": f64},
+                    "traffic": traffic.get("dopri_mix_kernel"), "kernel": "dopri_mix_kernel",
+                    "flops_per_step": f32, "flops_per_step_total": f64 + f32,
                     "attempted_steps_per_step": r["ode_steps"], "device_s_per_step": r["t_ode"],
-                    "peak_basis": ("measured: " + peaks["method"]) if peaks else
-                                  f"148 SM x 64 FP64 lanes x 2 x {sm_mhz:.0f} MHz",
+                    "peak_basis": basis32,
                     "timing": "CUDA events around every msgb_ode_trajectories call inside the timed steps; "
                               "attempted steps counted on the device"})
     out.sort(key=lambda e: -e["device_s_per_step"])

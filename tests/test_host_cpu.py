@@ -246,7 +246,8 @@ def test_bench_reports_the_dominant_kernel():
     """bench.py's roofline object is the kernel with the largest device time
     per step, with its algorithmic cost per work unit: the summation kernels
     (flops per evaluated triple, measured FP32 peak) and, in heterogeneous
-    media, the beam ODE (flops per attempted step, measured FP64 peak)."""
+    media, the FP32 path's mixed-precision beam ODE (FP32 flops per attempted
+    step against the FP32 peak, its FP64 ray flops against the FP64 peak)."""
     import types
 
     import bench
@@ -264,8 +265,11 @@ def test_bench_reports_the_dominant_kernel():
     assert bench.rooflines(r, peaks, 1965.0, args)[0]["kernel"] == "fwd32_kernel"
     r.update(hetero=True, t_ode=4.0, ode_steps=3e9)
     first, other = bench.rooflines(r, peaks, 1965.0, args)
-    assert first["kernel"] == "dopri_kernel" and first["bound"] == "fp64"
-    assert abs(first["frac"] - 3e9 * bench.ode_flops_per_step(2) / 4.0 / 1e12 / 36.0) < 1e-12
+    assert first["kernel"] == "dopri_mix_kernel" and first["bound"] == "fp32"
+    f64, f32 = bench.ode_flops_split(2)
+    assert f64 + f32 == bench.ode_flops_per_step(2) and 0 < f64 < f32
+    assert abs(first["frac"] - 3e9 * f32 / 4.0 / 1e12 / 72.0) < 1e-12
+    assert abs(first["fp64"]["frac"] - 3e9 * f64 / 4.0 / 1e12 / 36.0) < 1e-12
     assert [e["kernel"] for e in other] == ["fwd32_kernel<TRAJ>", "adj32_kernel<TRAJ>"]
 
 
