@@ -149,8 +149,15 @@ class Domain:
         Returns ``("constant", c)`` for a homogeneous medium and
         ``("grid", interpolant)`` for a grid-valued speed (n-linear, wrap
         boundary when every axis is periodic, clamp otherwise, as
-        geometry.py:191-203) or a ``GridInterpolant``.  Other callables are
-        only supported when they are constant on the grid.
+        geometry.py:191-203) or a ``GridInterpolant``.  Any other callable
+        c(x) (geometry.py:176-190 accepts one) is sampled once at the grid
+        nodes on the host and interpolated by the cubic B-spline of those
+        samples (same boundary rule): it equals c at every node and carries
+        the continuous gradient and Hessian the ray and Riccati equations
+        need; between nodes it differs from c by the interpolation error of
+        the samples.  The interpolant is built once per value of ``c`` and
+        reused, so the device caches and the kept trajectories key on one
+        object.
         """
         from .utils.interp import GridInterpolant, make_c_function_from_grid
 
@@ -159,12 +166,18 @@ class Domain:
             return "constant", c
         if isinstance(self.c, GridInterpolant):
             return "grid", self.c
+        cached = getattr(self, "_medium_cache", None)
+        if cached is not None and cached[0] is self.c:
+            return "grid", cached[1]
+        boundary = "wrap" if all(self.periodic) else "clamp"
         if not callable(self.c):
-            return "grid", make_c_function_from_grid(np.asarray(self.c, float), spacing=self.dx,
-                                                     origin=(0.0,) * self.ndim,
-                                                     boundary="wrap" if all(self.periodic) else "clamp")
-        raise NotImplementedError("a non-constant Python callable c(x) cannot be evaluated on the GPU; "
-                                  "use utils.interp.make_c_function_from_grid")
+            interp = make_c_function_from_grid(np.asarray(self.c, float), spacing=self.dx,
+                                               origin=(0.0,) * self.ndim, boundary=boundary)
+        else:
+            interp = make_c_function_from_grid(np.asarray(self.sound_speed_array, float), spacing=self.dx,
+                                               origin=(0.0,) * self.ndim, method="bspline3", boundary=boundary)
+        self._medium_cache = (self.c, interp)
+        return "grid", interp
 
     def constant_speed(self) -> Optional[float]:
         """The sound speed when the medium is homogeneous, else ``None``.

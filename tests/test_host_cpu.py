@@ -329,3 +329,21 @@ def test_problem_struct_owns_its_device_arrays():
     gc.collect()
     assert pr.ts == ptr and pr._owned[0].data_ptr() == ptr
     assert np.array_equal(pr._owned[0].numpy(), np.asarray(ts, np.float64))
+
+
+def test_callable_sound_speed_is_sampled_once_onto_a_bspline():
+    """A Python callable c(x) (geometry.py:176-190) becomes the cubic B-spline
+    of its grid samples: equal to c at every node, built once per value of
+    c (the device caches and kept trajectories key on that object)."""
+    dom = bb.Domain(N=(24, 20), dx=(1e-4, 2e-4), periodic=(False, False), cfl=0.3,
+                    c=lambda x: 1500.0 * (1.0 + 0.05 * np.sin(900.0 * x[..., 0]) * np.cos(700.0 * x[..., 1])))
+    kind, m = dom.medium()
+    assert kind == "grid" and m.method == "bspline3" and m.boundary == "nearest"  # clamp
+    assert dom.medium()[1] is m
+    xs = np.stack(np.meshgrid(np.arange(24) * 1e-4, np.arange(20) * 2e-4, indexing="ij"), -1)
+    ref = 1500.0 * (1.0 + 0.05 * np.sin(900.0 * xs[..., 0]) * np.cos(700.0 * xs[..., 1]))
+    assert np.allclose(np.asarray(m(xs.reshape(-1, 2))).reshape(24, 20), ref, rtol=1e-12, atol=1e-9)
+    const = bb.Domain(N=(8, 8), dx=(1e-4, 1e-4), periodic=(False, False), cfl=0.3, c=lambda x: 1480.0 + 0.0 * x[..., 0])
+    assert const.medium() == ("constant", 1480.0)
+    dom.c = lambda x: 1500.0 + 0.0 * x[..., 0] + 10.0 * x[..., 1]
+    assert dom.medium()[1] is not m
