@@ -1080,8 +1080,7 @@ class MSGBSolver:
         if cached is not None:
             sel_sorted = selection  # the order of the kept trajectory records
         else:
-            order = torch_argsort(selection.idx)
-            sel_sorted = Selection(selection.idx[order], selection.values[order], selection.total_coeffs)
+            sel_sorted = _sorted_selection(selection)
         bt = self.beams(sel_sorted, domain, wpt)
         if complex_data:
             g = self._gather_complex(bt, domain, sensors, ts, data)
@@ -1109,8 +1108,7 @@ class MSGBSolver:
         G = torch.zeros(wpt.total_coeffs, dtype=torch.complex128, device=dev)
         st = torch.cuda.current_stream(dev).cuda_stream
         for sel, modes in ((selection.pos, 1), (selection.neg, 2)):
-            order = torch_argsort(sel.idx)
-            s_sorted = Selection(sel.idx[order], sel.values[order], sel.total_coeffs)
+            s_sorted = _sorted_selection(sel)
             bt = replace(self.beams(s_sorted, domain, wpt), modes=modes)
             g = self._gather_complex(bt, domain, sensors, ts, data)
             _lib.check(_lib.lib().msgb_scatter_coeff_grad(s_sorted.idx.data_ptr(), torch.view_as_real(g).data_ptr(),
@@ -1390,6 +1388,18 @@ def torch_argsort(x):
     import torch
 
     return torch.argsort(x)
+
+
+def _sorted_selection(sel: Selection) -> Selection:
+    """The selection in ascending flat-index order, sorted once per
+    selection object (a frozen selection reused by many adjoints, as in a
+    reconstruction loop, is not sorted again)."""
+    cached = getattr(sel, "_sorted", None)
+    if cached is None or cached[0] is not sel.idx:
+        order = torch_argsort(sel.idx)
+        cached = (sel.idx, Selection(sel.idx[order], sel.values[order], sel.total_coeffs))
+        sel._sorted = cached
+    return cached[1]
 
 
 def _is_torch(x) -> bool:
