@@ -676,7 +676,9 @@ struct DopriMix {
     int code;
     double *k64;  // stage j, entry c at k64[(j ND + c) kst]
     float *k32;   // stage j, entry c at k32[(j NF + c) kst]
-    int kst;
+    // the block size (every integrator launch has 64 lanes): a compile-time
+    // stride turns the stage addresses into immediate offsets
+    static constexpr int kst = 64;
 
     __device__ void init(const MediumArgs &med, const ProbArgs &P, const OdeArgs &o, double mode_) {
         mode = mode_;
@@ -885,8 +887,7 @@ dopri_mix_kernel(ProbArgs P, MediumArgs med, BeamArgs B, TrajArgs T, OdeArgs o, 
     bool active = false;
     DopriMix<D, KIND> s;
     s.k64 = dopri_stage_smem + threadIdx.x;
-    s.k32 = reinterpret_cast<float *>(dopri_stage_smem + 7 * ND * blockDim.x) + threadIdx.x;
-    s.kst = blockDim.x;
+    s.k32 = reinterpret_cast<float *>(dopri_stage_smem + 7 * ND * DopriMix<D, KIND>::kst) + threadIdx.x;
     RecordWriter<D> rw(P, T, 0, 0.0, tt_len);
     unsigned long long lane_steps = 0;
     for (;;) {

@@ -67,15 +67,18 @@ def test_gemm_transposed_operands():
 
 def test_mlp_forward_backward_match_oracle():
     """Gradients of the hand-written backward against the FP64 oracle of the
-    same BF16 rounding points (oracle/mlp.py); 2e-3 relative per tensor."""
+    same BF16 rounding points (oracle/mlp.py); 2e-3 relative per tensor, and
+    the output within one BF16 unit in the last place of its largest entry (a
+    product that rounds to the other side of a BF16 value in one layer moves
+    the output by that much)."""
     from beamax_b200.surrogate import IN_PAD, MLP
     from oracle import mlp as orc
 
     dev = _dev()
     net = MLP(7, 12, width=256, depth=4, device=dev, seed=3)
-    for l in range(len(net.b)):  # non-zero biases exercise the bias path
-        net.b[l].normal_(0, 0.1)
     g = torch.Generator(device="cpu").manual_seed(1)
+    for l in range(len(net.b)):  # non-zero biases exercise the bias path (seeded)
+        net.b[l].copy_(0.1 * torch.randn(net.b[l].shape, generator=g))
     X = torch.zeros(384, IN_PAD)
     X[:, :7] = torch.randn(384, 7, generator=g)
     X16 = X.to(torch.bfloat16).to(dev)
@@ -86,7 +89,7 @@ def test_mlp_forward_backward_match_oracle():
     W = [w.cpu().numpy() for w in net.W]
     b = [x.cpu().numpy() for x in net.b]
     Zr, ar, pr = orc.forward(W, b, X16.float().cpu().numpy())
-    assert np.max(np.abs(out.cpu().numpy() - Zr)) <= 2e-3 * np.max(np.abs(Zr))
+    assert np.max(np.abs(out.cpu().numpy() - Zr)) <= 2.0 ** -8 * np.max(np.abs(Zr))
     gWr, gbr = orc.backward(W, ar, pr, dY.numpy())
     for l in range(len(W)):
         assert np.linalg.norm(gW[l].cpu().numpy() - gWr[l]) <= 2e-3 * np.linalg.norm(gWr[l]), l
