@@ -330,7 +330,6 @@ constexpr size_t dopri_mix_smem_bytes(int blk) {
     return (size_t)blk * 7 * (2 * D * sizeof(double) + (D * (D + 1) + 2) * sizeof(float));
 }
 constexpr int kMixBlocks = 6;  // default blocks per SM of the mixed-precision integrator (measured best at config 3)
-constexpr int kMixSpan = 1;    // default save times per step of the mixed-precision integrator
 
 // DENSE: save times may fall inside a step (msgb_ode_opts.dense_output);
 // without it every step ends on a save time and the continuous extension is
@@ -664,50 +663,10 @@ __constant__ float DP_E32[7] = {(float)(35.0 / 384 - 5179.0 / 57600),
                                 (float)(11.0 / 84 - 187.0 / 2100),
                                 (float)(-1.0 / 40)};
 
-// The continuous extension of a mixed-precision step at theta in (0, 1),
-// from the step's end points and its 7 stages (DopriBeam's dense output on
-// the FP64 ray and the FP32 Hessian and amplitude).  Not inlined: it runs for
-// the save times a step passes, and its registers stay off the step's path.
-template <int D>
-__device__ __noinline__ void mix_extension(const MState<D> &y, const MState<D> &yt, const double *k64,
-                                           const float *k32, double th, double hh, State<D> &out) {
-    constexpr int ND = MState<D>::ND, NF = MState<D>::NF, kst = 64;
-    MState<D> yd;
-#pragma unroll
-    for (int c = 0; c < ND; ++c) {
-        double r5 = 0.0;
-#pragma unroll
-        for (int j = 0; j < 7; ++j)
-            if (j != 1) r5 += DP_D[j] * k64[(j * ND + c) * kst];  // DP_D[1] = 0
-        r5 *= hh;
-        const double r2 = yt.r[c] - y.r[c];
-        const double r3 = hh * k64[c * kst] - r2;
-        const double r4 = r2 - hh * k64[(6 * ND + c) * kst] - r3;
-        yd.r[c] = y.r[c] + th * (r2 + (1.0 - th) * (r3 + th * (r4 + (1.0 - th) * r5)));
-    }
-    const float hf = (float)hh, thf = (float)th;
-#pragma unroll
-    for (int c = 0; c < NF; ++c) {
-        float r5 = 0.0f;
-#pragma unroll
-        for (int j = 0; j < 7; ++j)
-            if (j != 1) r5 = fmaf((float)DP_D[j], k32[(j * NF + c) * kst], r5);
-        r5 *= hf;
-        const float r2 = yt.f[c] - y.f[c];
-        const float r3 = fmaf(hf, k32[c * kst], -r2);
-        const float r4 = r2 - fmaf(hf, k32[(6 * NF + c) * kst], r3);
-        yd.f[c] = fmaf(thf, fmaf(1.0f - thf, fmaf(thf, fmaf(1.0f - thf, r5, r4), r3), r2), y.f[c]);
-    }
-    mix_to_full(yd, out);
-}
-
-// DopriBeam's step on the mixed state.  A step ends at most SPAN save times
-// ahead (landing on the SPAN-th); save times it passes are read from the
-// pair's 4th-order continuous extension (Shampine's weights, DP_D), as
-// DopriBeam's dense output does.  SPAN = 1: every step ends on a save time.
-// Stages in shared memory: the FP64 ray stages, then the FP32 Hessian and
-// amplitude stages, each entry strided by the block size.
-template <int D, int KIND, int SPAN = 1>
+// DopriBeam's step (save times landed on, no continuous extension) on the
+// mixed state.  Stages in shared memory: the FP64 ray stages, then the FP32
+// Hessian and amplitude stages, each entry strided by the block size.
+template <int D, int KIND>
 struct DopriMix {
     static constexpr int ND = MState<D>::ND, NF = MState<D>::NF, S = MState<D>::S;
     MState<D> y;
@@ -745,7 +704,7 @@ struct DopriMix {
             code = 2;
             return true;
         }
-        const double target = P.ts[(k + SPAN - 1 < P.nt - 1) ? k + SPAN - 1 : P.nt - 1];
+        const double target = P.ts[k];
         double hh = h;
         bool last = false;
         if (t + hh >= target) {
@@ -827,11 +786,7 @@ struct DopriMix {
             const double t_new = last ? target : t + hh;
             while (k < P.nt && P.ts[k] <= t_new) {
                 State<D> yf;
-                if (SPAN == 1 || P.ts[k] == t_new) {
-                    mix_to_full(yt, yf);
-                } else {
-                    mix_extension<D>(y, yt, k64, k32, (P.ts[k] - t) / hh, hh, yf);
-                }
+                mix_to_full(yt, yf);
                 rw.put(k, yf, false);
                 ++k;
             }
@@ -923,16 +878,16 @@ dopri_kernel(ProbArgs P, MediumArgs med, BeamArgs B, TrajArgs T, OdeArgs o, int 
 }
 
 // dopri_kernel with the FP32 path's mixed-precision state (DopriMix).
-template <int D, int KIND, int MINB, int SPAN>
+template <int D, int KIND, int MINB>
 __global__ void __launch_bounds__(64, MINB)
 dopri_mix_kernel(ProbArgs P, MediumArgs med, BeamArgs B, TrajArgs T, OdeArgs o, int tt_len) {
     constexpr int ND = MState<D>::ND;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     int64_t bl = blockIdx.x * (int64_t)blockDim.x + threadIdx.x - stride;
     bool active = false;
-    DopriMix<D, KIND, SPAN> s;
+    DopriMix<D, KIND> s;
     s.k64 = dopri_stage_smem + threadIdx.x;
-    s.k32 = reinterpret_cast<float *>(dopri_stage_smem + 7 * ND * DopriMix<D, KIND, SPAN>::kst) + threadIdx.x;
+    s.k32 = reinterpret_cast<float *>(dopri_stage_smem + 7 * ND * DopriMix<D, KIND>::kst) + threadIdx.x;
     RecordWriter<D> rw(P, T, 0, 0.0, tt_len);
     unsigned long long lane_steps = 0;
     for (;;) {
@@ -1071,18 +1026,15 @@ struct Dopri {
     int minb;
     bool f32m;   // FP32 path: FP32 medium, and without dense output the mixed-precision state
     bool dense;  // save times from the continuous extension
-    int span;    // mixed-precision state: save times one step may span
     bool mixed() const { return f32m && !dense; }
     template <int D, int K>
     auto kernel() const {
         if (dense) return f32m ? dopri_kernel<D, K, 4, true, true> : dopri_kernel<D, K, 4, false, true>;
-        if (f32m) {
-            if (minb >= 6)
-                return span >= 3 ? dopri_mix_kernel<D, K, 6, 3>
-                                 : (span == 2 ? dopri_mix_kernel<D, K, 6, 2> : dopri_mix_kernel<D, K, 6, 1>);
-            return span >= 3 ? dopri_mix_kernel<D, K, 4, 3>
-                             : (span == 2 ? dopri_mix_kernel<D, K, 4, 2> : dopri_mix_kernel<D, K, 4, 1>);
-        }
+        if (f32m)
+            return minb >= 7   ? dopri_mix_kernel<D, K, 7>
+                   : minb == 6 ? dopri_mix_kernel<D, K, 6>
+                   : minb == 5 ? dopri_mix_kernel<D, K, 5>
+                               : dopri_mix_kernel<D, K, 4>;
         return minb >= 5 ? dopri_kernel<D, K, 5, false, false> : dopri_kernel<D, K, 4, false, false>;
     }
     template <int D>
@@ -1095,20 +1047,9 @@ struct TrFinal {
     size_t smem() const { return dopri_smem_bytes<D>(64); }
 };
 
-// Save times one step of the mixed-precision integrator may span:
-// MSGB_DOPRI_SPAN (1 to 3), else kMixSpan.
-int dopri_span() {
-    static const int v = [] {
-        const char *e = getenv("MSGB_DOPRI_SPAN");
-        const int x = e ? atoi(e) : 0;
-        return (x >= 1 && x <= 3) ? x : kMixSpan;
-    }();
-    return v;
-}
-
 // Blocks of 64 lanes per SM of the adaptive integrator: MSGB_DOPRI_BLOCKS
 // (4 to 7; 5, 6 and 7 bound the registers to 204, 170 and 146; the FP64
-// integrator takes at most 5, the mixed-precision one 4 or 6), else `dflt`.
+// integrator takes at most 5), else `dflt`.
 int dopri_blocks_per_sm(int dflt) {
     static const int env = [] {
         const char *e = getenv("MSGB_DOPRI_BLOCKS");
@@ -1224,10 +1165,9 @@ extern "C" int msgb_ode_trajectories(const msgb_problem *prob, const msgb_medium
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         const bool f32m = opts->medium_fp32 != 0 && med->coeffs32 != nullptr && med->kind != MSGB_MEDIUM_CONSTANT;
-        Dopri which{4, f32m, opts->dense_output != 0, dopri_span()};
+        Dopri which{4, f32m, opts->dense_output != 0};
         which.minb = dopri_blocks_per_sm(which.mixed() ? kMixBlocks : 4);
         if (!which.mixed() && which.minb > 5) which.minb = 5;
-        if (which.mixed()) which.minb = which.minb >= 6 ? 6 : 4;
         {
             // the lanes are persistent: every block must be resident at once
             const size_t sm_bytes = prob->ndim == 1 ? which.smem<1>() : (prob->ndim == 2 ? which.smem<2>() : which.smem<3>());
