@@ -347,3 +347,24 @@ def test_callable_sound_speed_is_sampled_once_onto_a_bspline():
     assert const.medium() == ("constant", 1480.0)
     dom.c = lambda x: 1500.0 + 0.0 * x[..., 0] + 10.0 * x[..., 1]
     assert dom.medium()[1] is not m
+
+
+@pytest.mark.parametrize("workload", ["c2", "het512"])
+def test_bench_reference_arm_prints_the_contract_line(workload):
+    """`bench.py --impl reference` (the CPU restatement on a bounded beam
+    sample): one JSON line with the metric, a cpu_baseline describing the run
+    and an e2e object with no host-device copies."""
+    import json
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--workload", workload,
+                          "--cpu-sample", "2", "--steps", "1", "--warmup", "0"],
+                         capture_output=True, text=True, timeout=600, cwd=root, check=True).stdout
+    line = json.loads(out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["value"] > 0 and line["unit"] == "evals/s"
+    assert line["higher_is_better"] is True
+    cb = line["cpu_baseline"]
+    assert cb["value"] == line["value"] and cb["kind"] == "port" and cb["cores"] >= 1 and "2 of" in cb["sample"]
+    assert line["e2e"] == {"value": line["value"], "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
