@@ -646,32 +646,6 @@ __device__ void rhs_mix(const MediumArgs &med, double mode, const MState<D> &y, 
     dy.f[2 * S + 1] = fmaf(ar, fi, ai * fr);
 }
 
-// The Dormand-Prince tableau (DP_A) as a compile-time function, for stage
-// inputs unrolled with constant coefficients.
-__host__ __device__ constexpr double dp_a(int s, int j) {
-    return s == 1   ? (j == 0 ? 1.0 / 5 : 0.0)
-           : s == 2 ? (j == 0 ? 3.0 / 40 : j == 1 ? 9.0 / 40 : 0.0)
-           : s == 3 ? (j == 0 ? 44.0 / 45 : j == 1 ? -56.0 / 15 : j == 2 ? 32.0 / 9 : 0.0)
-           : s == 4 ? (j == 0   ? 19372.0 / 6561
-                       : j == 1 ? -25360.0 / 2187
-                       : j == 2 ? 64448.0 / 6561
-                       : j == 3 ? -212.0 / 729
-                                : 0.0)
-           : s == 5 ? (j == 0   ? 9017.0 / 3168
-                       : j == 1 ? -355.0 / 33
-                       : j == 2 ? 46732.0 / 5247
-                       : j == 3 ? 49.0 / 176
-                       : j == 4 ? -5103.0 / 18656
-                                : 0.0)
-           : s == 6 ? (j == 0   ? 35.0 / 384
-                       : j == 2 ? 500.0 / 1113
-                       : j == 3 ? 125.0 / 192
-                       : j == 4 ? -2187.0 / 6784
-                       : j == 5 ? 11.0 / 84
-                                : 0.0)
-                    : 0.0;
-}
-
 __constant__ float DP_A32[7][6] = {
     {0, 0, 0, 0, 0, 0},
     {(float)(1.0 / 5), 0, 0, 0, 0, 0},
@@ -722,33 +696,6 @@ struct DopriMix {
         for (int c = 0; c < NF; ++c) k32[c * kst] = f0.f[c];
     }
 
-    // y + hh sum_j a_sj k_j for stage s = SS (row SS of the tableau, dp_a)
-    template <int SS>
-    __device__ __forceinline__ void stage_input(double hh, float hf, MState<D> &yt) const {
-        double a64[ND];
-        float a32[NF];
-#pragma unroll
-        for (int c = 0; c < ND; ++c) a64[c] = 0.0;
-#pragma unroll
-        for (int c = 0; c < NF; ++c) a32[c] = 0.0f;
-#pragma unroll
-        for (int j = 0; j < SS; ++j) {
-            constexpr double kRow[6] = {dp_a(SS, 0), dp_a(SS, 1), dp_a(SS, 2), dp_a(SS, 3), dp_a(SS, 4), dp_a(SS, 5)};
-            const double a = kRow[j];
-            if (a != 0.0) {
-                const float af = (float)a;
-#pragma unroll
-                for (int c = 0; c < ND; ++c) a64[c] += a * k64[(j * ND + c) * kst];
-#pragma unroll
-                for (int c = 0; c < NF; ++c) a32[c] = fmaf(af, k32[(j * NF + c) * kst], a32[c]);
-            }
-        }
-#pragma unroll
-        for (int c = 0; c < ND; ++c) yt.r[c] = y.r[c] + hh * a64[c];
-#pragma unroll
-        for (int c = 0; c < NF; ++c) yt.f[c] = fmaf(hf, a32[c], y.f[c]);
-    }
-
     __device__ bool attempt(const MediumArgs &med, const ProbArgs &P, const OdeArgs &o, RecordWriter<D> &rw) {
         constexpr int NE = 2 * D + S + 1;          // entries of the error norm (x, p real; M, A complex)
         constexpr int NE_FULL = 2 * D + D * D + 1;  // entries of the full state
@@ -768,16 +715,27 @@ struct DopriMix {
         MState<D> yt;
 #pragma unroll 1
         for (int s = 1; s < 7; ++s) {
-            // stage s's input, its coefficients compile-time constants (one
-            // branch per stage instead of a loop over the tableau row)
-            switch (s) {
-                case 1: stage_input<1>(hh, hf, yt); break;
-                case 2: stage_input<2>(hh, hf, yt); break;
-                case 3: stage_input<3>(hh, hf, yt); break;
-                case 4: stage_input<4>(hh, hf, yt); break;
-                case 5: stage_input<5>(hh, hf, yt); break;
-                default: stage_input<6>(hh, hf, yt); break;
+            double a64[ND];
+            float a32[NF];
+#pragma unroll
+            for (int c = 0; c < ND; ++c) a64[c] = 0.0;
+#pragma unroll
+            for (int c = 0; c < NF; ++c) a32[c] = 0.0f;
+#pragma unroll 1
+            for (int j = 0; j < s; ++j) {
+                const double a = DP_A[s][j];
+                if (a != 0.0) {
+                    const float af = DP_A32[s][j];
+#pragma unroll
+                    for (int c = 0; c < ND; ++c) a64[c] += a * k64[(j * ND + c) * kst];
+#pragma unroll
+                    for (int c = 0; c < NF; ++c) a32[c] = fmaf(af, k32[(j * NF + c) * kst], a32[c]);
+                }
             }
+#pragma unroll
+            for (int c = 0; c < ND; ++c) yt.r[c] = y.r[c] + hh * a64[c];
+#pragma unroll
+            for (int c = 0; c < NF; ++c) yt.f[c] = fmaf(hf, a32[c], y.f[c]);
             MState<D> kn;
             rhs_mix<D, KIND>(med, mode, yt, kn);
 #pragma unroll
