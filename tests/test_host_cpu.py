@@ -368,3 +368,32 @@ def test_bench_reference_arm_prints_the_contract_line(workload):
     cb = line["cpu_baseline"]
     assert cb["value"] == line["value"] and cb["kind"] == "port" and cb["cores"] >= 1 and "2 of" in cb["sample"]
     assert line["e2e"] == {"value": line["value"], "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_compact_store_layout_stays_inside_its_buffer():
+    """The compact trajectory store's slot table, block counter, culling boxes
+    and record pool, as _compact_tr lays them out in one buffer: disjoint,
+    aligned, and inside the buffer for every buffer size (the device kernels
+    index them without a bounds check beyond pool_blocks)."""
+    torch = pytest.importorskip("torch")
+    s = bb.MSGBSolver(64, "top_n", 16, "spatial", bb.gb.gb_solvers.solve_ODE_base, "scan_real", precision="fp32")
+    rng = np.random.default_rng(0)
+    for _ in range(200):
+        d = int(rng.integers(1, 4))
+        nt = int(rng.integers(1, 6000))
+        nb = int(rng.integers(1, 5000))
+        n_tt, block, cull = s._compact_sizes(d, nt)
+        size = int(rng.integers(n_tt * nb * 4 + 1024, n_tt * nb * 4 + 2048 + 200 * (block + cull)))
+        buf = torch.empty(size, dtype=torch.uint8)
+        status = torch.zeros(nb + 8, dtype=torch.int32)
+        boxes = torch.zeros((4, 2 * d), dtype=torch.float32)
+        tr, blocks, ctr = s._compact_tr(buf, d, nt, 3, nb, status, boxes, 4)
+        base = buf.data_ptr()
+        slot_end = tr.slot - base + n_tt * nb * 4
+        ctr_off, cull_off, pool_off = tr.pool_next - base, tr.pool_cull - base, tr.pool - base
+        assert tr.slot == base and slot_end <= ctr_off and ctr_off + 8 <= cull_off
+        assert blocks >= 0 and tr.pool_blocks == blocks
+        assert cull_off + blocks * cull <= pool_off and pool_off % 256 == 0
+        assert pool_off + blocks * block <= size
+        assert ctr.numel() == 1 and ctr.data_ptr() == tr.pool_next
+        assert tr.status == status.data_ptr() + 4 * 3 and tr.nb == nb and tr.b_first == 3
