@@ -249,10 +249,14 @@ typedef struct msgb_ode_opts {
                                 control and save times come from the continuous extension */
     unsigned long long *step_count; /* optional device counter (NULL: none): attempted
                                 DOPRI5 steps (accepted + rejected) of the call are added to it */
-    int32_t medium_fp32;     /* DOPRI5 with a grid medium and med->coeffs32: evaluate c, grad c
-                                and hess c in FP32 (taps centred on the nearest one, result
-                                + c_ref in FP64); the ray, Riccati and amplitude stay FP64.
-                                For the FP32 path; the FP64 path evaluates in FP64. */
+    int32_t medium_fp32;     /* DOPRI5 with a grid medium and med->coeffs32, for the FP32 path:
+                                evaluate c, grad c and hess c in FP32 (taps centred on the
+                                nearest one, result + c_ref in FP64) and form the step-size
+                                error norm in FP32.  Without dense_output the Hessian M and
+                                the amplitude A are also integrated in FP32 (the ray x, p
+                                stays FP64): the mixed-precision integrator, whose FP32
+                                rounding stays far below the FP32 summation's.  0: every
+                                operation in FP64 (the FP64 path). */
 } msgb_ode_opts;
 
 /* FP64 integration of coupled_rhs_absorption (gb/gb_solvers.py:787-867) for
