@@ -268,6 +268,8 @@ def test_bench_reports_the_dominant_kernel():
     assert first["kernel"] == "dopri_mix_kernel" and first["bound"] == "fp32"
     f64, f32 = bench.ode_flops_split(2)
     assert f64 + f32 == bench.ode_flops_per_step(2) and 0 < f64 < f32
+    f64_3, f32_3 = bench.ode_flops_split(3)
+    assert f64_3 + f32_3 == bench.ode_flops_per_step(3) and 0 < f64_3 < f32_3
     assert abs(first["frac"] - 3e9 * f32 / 4.0 / 1e12 / 72.0) < 1e-12
     assert abs(first["fp64"]["frac"] - 3e9 * f64 / 4.0 / 1e12 / 36.0) < 1e-12
     assert [e["kernel"] for e in other] == ["fwd32_kernel<TRAJ>", "adj32_kernel<TRAJ>"]
