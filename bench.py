@@ -9,7 +9,8 @@ correlation length clipped to [-1, 1] (cubic B-spline interpolant), cfl 0.3
 rectangular_mirror (the stated 5-level tiling is rejected by the reference's
 own validation); p0 = 256 seeded Gaussian wave packets + 8 blobs, max|p0| = 1;
 four-sided line sensor (4092 points); thr = 262144 top_n (524288 beams);
-adaptive FP64 beam ODE (Dormand-Prince 5(4), rtol 1e-7, atol 1e-9).
+adaptive beam ODE (Dormand-Prince 5(4), rtol 1e-7, atol 1e-9; FP64 ray, FP32
+Hessian and amplitude on the FP32 path, all FP64 on the FP64 path).
 Synthetic seeded data of those shapes; nothing is downloaded.
 
 A step = one forward (p0 -> sensor data) plus one exact adjoint (data ->

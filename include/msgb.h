@@ -559,7 +559,7 @@ int msgb_scatter_coeff_grad(const int64_t *idx, const double *g, int64_t n, doub
                             msgb_stream_t stream);
 
 /* ---- throughput probes (measurement; no counterpart in the reference) ---
- * The roofline denominators of the FP32 summation, the FP64 beam ODE and the
+ * The roofline denominators of the FP32 summation, the beam ODE (FP32 and FP64) and the
  * special-function unit, measured on the device that runs them: blocks x
  * threads threads each run 8 independent chains of `iters` operations of one
  * kind.  The caller times the launch on its stream and divides
